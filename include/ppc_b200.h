@@ -1,0 +1,152 @@
+/* C ABI of the B200 photon propagator (libppcb.so).
+ *
+ * Plain pointers and sizes only.  Every call returns 0 on success or a nonzero status
+ * (PPCB_E*) with a message from ppcb_last_error(); where the reference calls exit(n)
+ * (gpu/ini.cxx passim, gpu/ppc.cu:98, :266, :505, gpu/f2k.cxx:533) the status is n.
+ *
+ * The functions mirror the reference's library interface, the xppc:: namespace of
+ * llh/ppc.h (defined in gpu/ppc.cu and gpu/f2k.cxx under -DXLIB); each cites the
+ * reference entry point it replaces.  A context holds what the reference keeps in
+ * globals (tables, device buffers, pending bunches, segment list, hit map), so several
+ * contexts may coexist in one process; one context must not be used from two host
+ * threads at once.  The record types are in ppc_b200/csrc/ppcb_types.h.
+ */
+#ifndef PPC_B200_H
+#define PPC_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../ppc_b200/csrc/ppcb_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPCB_OK 0
+#define PPCB_ECONFIG 1    /* bad or missing input file (reference: exit(1)) */
+#define PPCB_ECUDA 2      /* CUDA runtime error (reference: exit(2)) */
+#define PPCB_ESEGMENT 3   /* too many event segments (reference: exit(3)) */
+#define PPCB_ESTATE 6     /* call out of order (e.g. propagation before ppcb_ini) */
+#define PPCB_EARG 7       /* invalid argument */
+#define PPCB_ENODEV 5     /* no usable GPU (reference: exit(5)) */
+
+typedef struct ppcb_ctx ppcb_ctx;
+
+/* One entry of the binned hit map (reference `hitz`, gpu/f2k.cxx:183-221), flattened:
+ * key fields (track, module, pmt, direction bin, time bin) followed by the photon. */
+typedef struct ppcb_hitz_rec {
+  int32_t track_first;
+  int32_t frame;
+  uint64_t track_second;
+  double t0;
+  int32_t str, om, pmt;
+  float dir, time;
+  float r[4], n[4];
+} ppcb_hitz_rec;
+
+typedef struct ppcb_run_info {
+  uint64_t photons;     /* photons propagated */
+  uint64_t hits;        /* kernel-level hits produced */
+  uint64_t kept;        /* hits stored (bounded by capacity) */
+  uint64_t steps;       /* propagation steps (scattering segments) */
+  uint32_t nan_steps;   /* steps with non-finite optical depth, photon dropped */
+  uint32_t capped;      /* photons stopped by the step cap */
+  double device_ms;     /* device time of the launches */
+} ppcb_run_info;
+
+typedef struct ppcb_info {
+  uint64_t max_bunch_size;   /* getMaxBunchSize(), gpu/ppc.cu:368 */
+  uint64_t workgroup_size;   /* getWorkgroupSize(), gpu/ppc.cu:370-386 */
+  double total_device_ms;    /* getTotalDeviceTime(), gpu/ppc.cu:388-395 */
+  uint64_t max_photons;      /* photons per launch (pmax) */
+  uint64_t hit_capacity;     /* hits per launch and device */
+  int32_t devices;
+  int32_t threads;           /* threads (= random streams) per device */
+  int32_t blocks;
+  int32_t regs;              /* registers per thread of the propagation kernel */
+  int32_t gsize, size, nstr, rsize;
+  float eff;                 /* photons per metre after acceptance (ppm) */
+  uint32_t ovr;              /* oversize area factor xR^2 */
+  uint32_t seed;
+  int32_t nextgen;
+} ppcb_info;
+
+const char* ppcb_last_error(void);
+
+/* ---- lifecycle ---- */
+int ppcb_create(ppcb_ctx** out);                                     /* start(), gpu/ppc.cu:481-483 */
+int ppcb_destroy(ppcb_ctx* c);                                       /* stop(), gpu/ppc.cu:485-488 */
+int ppcb_initialize(ppcb_ctx* c, const char* tables_dir, float enh); /* initialize(), gpu/ppc.cu:36; dir NULL: PPCTABLESDIR */
+int ppcb_choose(ppcb_ctx* c, int device);                            /* choose(), gpu/ppc.cu:490-508 */
+int ppcb_set_seed(ppcb_ctx* c, uint32_t seed);                       /* fixed seed instead of the clock (gpu/ini.cxx:792-795, DTMN) */
+int ppcb_set_options(ppcb_ctx* c, int deterministic, uint32_t max_steps, int blocks_per_sm);
+int ppcb_ini(ppcb_ctx* c);                                           /* ini(), gpu/ppc.cu:330-361 */
+int ppcb_fin(ppcb_ctx* c);                                           /* fin(), gpu/ppc.cu:398-402 */
+int ppcb_get_info(ppcb_ctx* c, ppcb_info* out);
+
+/* ---- sources ---- */
+int ppcb_flset(ppcb_ctx* c, int str, int om, ppcb_dom* out);         /* flset(), gpu/f2k.cxx:630-759 */
+int ppcb_fldir(ppcb_ctx* c, float dir[3]);                           /* fldir(), gpu/f2k.cxx:762-765 */
+int ppcb_flshift(ppcb_ctx* c, float m[3], float n[3], float* r);     /* flshift(), gpu/f2k.cxx:590-628; r may be NULL */
+int ppcb_sett(ppcb_ctx* c, float nx, float ny, float nz, int32_t id_first, uint64_t id_second, int32_t frame,
+              double t0);                                            /* sett(), gpu/f2k.cxx:548-552 */
+int ppcb_addp(ppcb_ctx* c, float x, float y, float z, float t, float E, float dr, int32_t type,
+              float scale);                                          /* addp(), gpu/f2k.cxx:484-504 */
+int ppcb_addp_clst(ppcb_ctx* c, float x, float y, float z, float t, uint64_t n, float dr,
+                   float beta);                                      /* addp_clst(), gpu/f2k.cxx:507-518 */
+int ppcb_addp_mopo(ppcb_ctx* c, float x, float y, float z, float t, float light, float length, float beta,
+                   float tau, float fr);                             /* addp_mopo(), gpu/f2k.cxx:520-528 */
+int ppcb_flone(ppcb_ctx* c, uint64_t num);                           /* flone(), gpu/f2k.cxx:586-588 */
+int ppcb_eout(ppcb_ctx* c);                                          /* eout(), gpu/f2k.cxx:536-541 */
+int ppcb_efin(ppcb_ctx* c);                                          /* efin(), gpu/f2k.cxx:544-546 */
+int ppcb_set_res(ppcb_ctx* c, float t, float cz);                    /* set_res(), gpu/f2k.cxx:202-210 */
+float ppcb_xrnd(ppcb_ctx* c);                                        /* xrnd(), gpu/f2k.cxx:1-6 */
+
+/* ---- results ---- */
+int ppcb_hitz_count(ppcb_ctx* c, uint64_t* records);                 /* hitz, gpu/f2k.cxx:221 */
+int ppcb_hitz_copy(ppcb_ctx* c, ppcb_hitz_rec* out, uint64_t cap, uint64_t* written);
+int ppcb_keep_raw(ppcb_ctx* c, int keep);                            /* also keep kernel-level hits */
+int ppcb_raw_count(ppcb_ctx* c, uint64_t* n);
+int ppcb_raw_copy(ppcb_ctx* c, ppcb_hit* out, uint64_t cap, uint64_t* written);
+int ppcb_last_run(ppcb_ctx* c, ppcb_run_info* last, ppcb_run_info* total);
+
+/* ---- the hot path, called directly ----
+ * ppcb_propagate: host buffers in and out (copies included).  Propagates the photons of
+ * `nb` bunches (photon counts in .num, segment ids in .q), in launches of at most
+ * max_photons, and writes kernel-level hits to `hits` (at most `cap`; *nhits receives
+ * the number produced, which may be larger).  Replaces the reference's kernel()
+ * (gpu/ppc.cu:432-469) with the front and back ends left out. */
+int ppcb_propagate(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, ppcb_hit* hits, uint64_t cap,
+                   uint64_t* nhits, ppcb_run_info* info);
+/* ppcb_propagate_device: one asynchronous launch on device `device` (index into the
+ * chosen devices) over caller-owned device memory, on `stream` (a cudaStream_t, NULL for
+ * the default stream).  bstart[k] is the first photon index of bunch k, bstart[nb] = num.
+ * `ctrl` must be zeroed before the launch; afterwards ctrl->hidx is the number of hits
+ * produced (only the first hcap are stored).  Replaces the main propagate launch,
+ * gpu/ppc.cu:293-306. */
+int ppcb_propagate_device(ppcb_ctx* c, int device, const ppcb_bunch* bunches, const uint64_t* bstart, int32_t nb,
+                          uint64_t num, ppcb_hit* hits, uint64_t hcap, ppcb_ctrl* ctrl, void* stream);
+/* Random stream state per thread (the reference keeps it in datz.rs, gpu/pro.cu:891-892):
+ * read or restore it, e.g. to checkpoint and resume a run.  n = threads of the device. */
+int ppcb_rng_get(ppcb_ctx* c, int device, uint64_t* rs, uint64_t n);
+int ppcb_rng_set(ppcb_ctx* c, int device, const uint64_t* rs, uint64_t n);
+int ppcb_rng_reset(ppcb_ctx* c);                                     /* rs_ini(), gpu/ini.cxx:556-571 */
+
+/* ---- inspection (tests, tools) ---- */
+/* Host copy of a named table (params, az, lr, ls, is, mcol, sc, lp, absca, wmeta, oms, rm,
+ * wvs, eff): pointer valid until the next ppcb_initialize / ppcb_destroy. */
+int ppcb_table(ppcb_ctx* c, const char* name, const void** ptr, uint64_t* bytes);
+/* Phase-1 sampling only: thread t samples photon t (t < num) with its own stream;
+ * out[3t..3t+2] = position, direction, (wavelength bin, segment, fla, ofla) as int bits. */
+int ppcb_generate_device(ppcb_ctx* c, int device, const ppcb_bunch* bunches, const uint64_t* bstart, int32_t nb,
+                         uint64_t num, void* out, void* stream);
+/* Index helpers at points: pos[2k] = (x,y,z,t), pos[2k+1] = (nx,ny,nz,length).
+ * out_i[8k..] = layer, cell x lo/hi, cell y lo/hi, DOM window lo/hi, string; out_f[2k..] =
+ * tilt shift, layer thickness (gpu/pro.cu:168-264, :507-515, :580-594, :623-626). */
+int ppcb_index_probe_device(ppcb_ctx* c, int device, const void* pos, int32_t n, int32_t* out_i, float* out_f,
+                            void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

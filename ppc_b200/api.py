@@ -1,0 +1,206 @@
+"""Python face of the propagator, mirroring the reference's library interface
+(namespace xppc in llh/ppc.h; definitions in gpu/ppc.cu and gpu/f2k.cxx) over the C ABI.
+
+    ctx = PPC()                       # start()
+    ctx.initialize(1.0, "ice/dir")    # initialize(enh); directory or PPCTABLESDIR
+    ctx.choose(0); ctx.ini()          # choose(device), ini()
+    ctx.flset(63, 20)                 # flset(str, om)
+    ctx.sett(0, 0, 1, (1, 7), 0)      # sett(nx, ny, nz, id, frame)
+    ctx.flone(10**7); ctx.eout()      # flone(num), eout()
+    ctx.hitz()                        # the binned hit map, flattened
+    ctx.efin(); ctx.fin()             # efin(), fin()
+
+Errors raise PPCError with the reference's exit status as `.code`.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import types as T
+from ._lib import HITZ_DTYPE, Dom, Info, PPCError, RunInfo, check, lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class PPC:
+    def __init__(self):
+        self._c = C.c_void_p()
+        check(lib().ppcb_create(C.byref(self._c)))
+
+    # ---- lifecycle -------------------------------------------------------------
+    def initialize(self, enh=1.0, tables_dir=None):
+        check(lib().ppcb_initialize(self._c, tables_dir.encode() if tables_dir else None, float(enh)))
+
+    def choose(self, device=0):
+        check(lib().ppcb_choose(self._c, int(device)))
+
+    def set_seed(self, seed):
+        check(lib().ppcb_set_seed(self._c, int(seed) & 0xFFFFFFFF))
+
+    def set_options(self, deterministic=False, max_steps=0, blocks_per_sm=0):
+        check(lib().ppcb_set_options(self._c, int(bool(deterministic)), int(max_steps), int(blocks_per_sm)))
+
+    def ini(self):
+        check(lib().ppcb_ini(self._c))
+
+    def fin(self):
+        check(lib().ppcb_fin(self._c))
+
+    def close(self):
+        if self._c:
+            lib().ppcb_destroy(self._c)
+            self._c = C.c_void_p()
+
+    stop = close
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        i = Info()
+        check(lib().ppcb_get_info(self._c, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in Info._fields_}
+
+    def getMaxBunchSize(self):
+        return self.info()["max_bunch_size"]
+
+    def getWorkgroupSize(self):
+        return self.info()["workgroup_size"]
+
+    def getTotalDeviceTime(self):
+        return self.info()["total_device_ms"]
+
+    # ---- sources -------------------------------------------------------------------
+    def flset(self, str_, om):
+        d = Dom()
+        check(lib().ppcb_flset(self._c, int(str_), int(om), C.byref(d)))
+        return {"R": d.R, "F": d.F, "r": list(d.r)}
+
+    def fldir(self):
+        a = np.zeros(3, np.float32)
+        check(lib().ppcb_fldir(self._c, _p(a)))
+        return a
+
+    def flshift(self, m, n, r=None):
+        m = np.ascontiguousarray(m, np.float32).copy()
+        n = np.ascontiguousarray(n, np.float32).copy()
+        rr = None if r is None else np.ascontiguousarray(r, np.float32).copy()
+        check(lib().ppcb_flshift(self._c, _p(m), _p(n), _p(rr)))
+        return (n, rr) if r is not None else n
+
+    def sett(self, nx, ny, nz, id_, frame, t0=0.0):
+        check(lib().ppcb_sett(self._c, nx, ny, nz, int(id_[0]), int(id_[1]), int(frame), float(t0)))
+
+    def addp(self, x, y, z, t, E, dr, type_, scale=1.0):
+        check(lib().ppcb_addp(self._c, x, y, z, t, E, dr, int(type_), scale))
+
+    def addp_clst(self, x, y, z, t, n, dr, beta):
+        check(lib().ppcb_addp_clst(self._c, x, y, z, t, int(n), dr, beta))
+
+    def addp_mopo(self, x, y, z, t, light, length, beta, tau, fr):
+        check(lib().ppcb_addp_mopo(self._c, x, y, z, t, light, length, beta, tau, fr))
+
+    def flone(self, num):
+        check(lib().ppcb_flone(self._c, int(num)))
+
+    def eout(self):
+        check(lib().ppcb_eout(self._c))
+
+    def efin(self):
+        check(lib().ppcb_efin(self._c))
+
+    def set_res(self, t, c=0.0):
+        check(lib().ppcb_set_res(self._c, float(t), float(c)))
+
+    def xrnd(self):
+        return lib().ppcb_xrnd(self._c)
+
+    # ---- results -------------------------------------------------------------------
+    def hitz(self):
+        n = C.c_uint64()
+        check(lib().ppcb_hitz_count(self._c, C.byref(n)))
+        out = np.zeros(n.value, HITZ_DTYPE)
+        w = C.c_uint64()
+        check(lib().ppcb_hitz_copy(self._c, _p(out), n.value, C.byref(w)))
+        return out
+
+    def keep_raw(self, keep=True):
+        check(lib().ppcb_keep_raw(self._c, int(bool(keep))))
+
+    def raw_hits(self):
+        n = C.c_uint64()
+        check(lib().ppcb_raw_count(self._c, C.byref(n)))
+        out = np.zeros(n.value, T.HIT_DTYPE)
+        w = C.c_uint64()
+        check(lib().ppcb_raw_copy(self._c, _p(out), n.value, C.byref(w)))
+        return out
+
+    def last_run(self):
+        a, b = RunInfo(), RunInfo()
+        check(lib().ppcb_last_run(self._c, C.byref(a), C.byref(b)))
+        f = lambda r: {k: getattr(r, k) for k, _ in RunInfo._fields_}
+        return f(a), f(b)
+
+    # ---- direct hot path -----------------------------------------------------------
+    def propagate(self, bunches, cap=1 << 22):
+        """Host bunches in, kernel-level hits out (copies included)."""
+        bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
+        hits = np.zeros(cap, T.HIT_DTYPE)
+        nh = C.c_uint64()
+        info = RunInfo()
+        check(lib().ppcb_propagate(self._c, _p(bunches), len(bunches), _p(hits), cap, C.byref(nh), C.byref(info)))
+        return hits[:min(nh.value, cap)], {k: getattr(info, k) for k, _ in RunInfo._fields_}
+
+    def propagate_device(self, bunches_ptr, bstart_ptr, nb, num, hits_ptr, hcap, ctrl_ptr, stream=0, device=0):
+        """One asynchronous launch over caller-owned device memory (raw pointers)."""
+        check(lib().ppcb_propagate_device(self._c, device, C.c_void_p(bunches_ptr), C.c_void_p(bstart_ptr), nb,
+                                          num, C.c_void_p(hits_ptr), hcap, C.c_void_p(ctrl_ptr),
+                                          C.c_void_p(stream) if stream else None))
+
+    def generate_device(self, bunches_ptr, bstart_ptr, nb, num, out_ptr, stream=0, device=0):
+        check(lib().ppcb_generate_device(self._c, device, C.c_void_p(bunches_ptr), C.c_void_p(bstart_ptr), nb, num,
+                                         C.c_void_p(out_ptr), C.c_void_p(stream) if stream else None))
+
+    def index_probe_device(self, pos_ptr, n, oi_ptr, of_ptr, stream=0, device=0):
+        check(lib().ppcb_index_probe_device(self._c, device, C.c_void_p(pos_ptr), n, C.c_void_p(oi_ptr),
+                                            C.c_void_p(of_ptr), C.c_void_p(stream) if stream else None))
+
+    def rng_get(self, device=0):
+        n = self.info()["threads"]
+        a = np.zeros(n, np.uint64)
+        check(lib().ppcb_rng_get(self._c, device, _p(a), n))
+        return a
+
+    def rng_set(self, rs, device=0):
+        rs = np.ascontiguousarray(rs, np.uint64)
+        check(lib().ppcb_rng_set(self._c, device, _p(rs), len(rs)))
+
+    def rng_reset(self):
+        check(lib().ppcb_rng_reset(self._c))
+
+    # ---- tables --------------------------------------------------------------------
+    def table(self, name):
+        ptr = C.c_void_p()
+        n = C.c_uint64()
+        check(lib().ppcb_table(self._c, name.encode(), C.byref(ptr), C.byref(n)))
+        return bytes(C.string_at(ptr, n.value)) if n.value else b""
+
+    def params(self):
+        p = T.Params()
+        C.memmove(C.byref(p), self.table("params"), C.sizeof(p))
+        return p
+
+    def tables(self):
+        """The kernel-facing table image as numpy arrays (copies)."""
+        b = lambda k, dt: np.frombuffer(self.table(k), dt).copy()
+        return {
+            "az": b("az", "<f4"), "lr": b("lr", "<f4"), "ls": b("ls", "<u2"), "is": b("is", "<u2"),
+            "mcol": b("mcol", "<i1"), "sc": b("sc", T.LINE_DTYPE), "lp": b("lp", "<f4"),
+            "absca": b("absca", "<f4"), "wmeta": b("wmeta", "<f4"), "oms": b("oms", T.DOM_DTYPE),
+            "rm": b("rm", "<u4"), "wvs": b("wvs", "<f4"), "eff": b("eff", "<f4"),
+        }

@@ -1,0 +1,111 @@
+// Device runtime: per-GPU table image in HBM, random streams, double-buffered launch
+// slots, hit collection.  Replaces the reference's `struct gpu` and kernel()
+// (gpu/ppc.cu:102-321, :432-469) with a depth-2 pipeline: batch k is queued before the
+// host waits for batch k-1, so the GPU is never idle between batches.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <deque>
+#include <string>
+#include <vector>
+
+#include "config.h"
+#include "propagate.cuh"
+
+namespace ppcb {
+
+struct RunInfo {
+  uint64_t photons = 0;
+  uint64_t hits = 0;        // produced by the kernel (may exceed what was kept)
+  uint64_t kept = 0;        // stored (bounded by the hit-buffer capacity)
+  uint64_t steps = 0;
+  uint32_t nan_steps = 0;
+  uint32_t capped = 0;
+  float device_ms = 0;
+  bool overflow = false;
+};
+
+struct DeviceCtx {
+  int dev = -1;
+  cudaDeviceProp prop{};
+  cudaStream_t st = nullptr, cp = nullptr;
+  LaunchShape shape{0, 0};
+  int T = 0;                      // threads in flight (= random streams)
+  // table image
+  float2* absca = nullptr;
+  ppcb_wmeta* wmeta = nullptr;
+  float2* lp = nullptr;
+  ppcb_dom* oms = nullptr;
+  ppcb_aniz* az = nullptr;
+  ppcb_line* sc = nullptr;
+  float* lr = nullptr;
+  uint16_t* ls = nullptr;
+  uint16_t* is = nullptr;
+  int8_t* mcol = nullptr;
+  uint64_t* rs = nullptr;
+  uint32_t* rm = nullptr;
+  struct Slot {
+    ppcb_bunch* bunches = nullptr;   // device
+    uint64_t* bstart = nullptr;      // device
+    ppcb_bunch* hb = nullptr;        // pinned staging
+    uint64_t* hbstart = nullptr;     // pinned staging
+    ppcb_hit* hits = nullptr;        // device
+    ppcb_ctrl* ctrl = nullptr;       // device
+    ppcb_ctrl* hctrl = nullptr;      // pinned
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    uint64_t num = 0;
+    int nb = 0;
+    bool busy = false;
+    long tag = 0;
+  } slot[2];
+  int next_slot = 0;
+  uint64_t bcap = 0, hcap = 0;
+  double device_ms = 0;
+  ppcb_hit* hhits = nullptr;       // pinned, grows
+  uint64_t hhits_cap = 0;
+};
+
+class Engine {
+ public:
+  ~Engine();
+  Config cfg;
+  unsigned int sv = 0;             // seed: MWC stream start and host rand_r state
+  bool deterministic = false;
+  uint32_t max_steps = 0;
+  std::vector<DeviceCtx> devs;
+  uint64_t pmax = 0, pmxo = 0;     // photons / bunches per launch
+  unsigned int hquo = 1;
+  int blocks_per_sm = 0;           // 0: occupancy maximum
+
+  void initialize(const std::string& dir, float enh);
+  void choose(int device);         // -1: every visible device
+  void ini();
+  void fin();
+  bool ready() const { return inited_; }
+
+  // Queue one batch (bunch list with photon counts) on every device; the photon range
+  // is split across devices in proportion to capacity (gpu/ppc.cu:313-320, :450-457).
+  long submit(const ppcb_bunch* b, int nb, uint64_t num);
+  // Wait for the oldest queued batch; append its kept hits.  False if none queued.
+  bool collect(std::vector<ppcb_hit>& out, RunInfo& info, long* tag = nullptr);
+  int in_flight() const { return (int)queue_.size(); }
+
+  // Device-pointer entry point: one launch on device `d` over caller buffers.
+  void launch_device(int d, const ppcb_bunch* dbunch, const uint64_t* dbstart, int nb, uint64_t num,
+                     ppcb_hit* dhits, uint64_t hcap, ppcb_ctrl* dctrl, cudaStream_t st);
+  void reset_streams();            // re-seed every stream (reference rs_ini, gpu/ini.cxx:556-571)
+  double total_device_ms() const;
+  KArgs args_for(int d) const;
+
+ private:
+  void free_device(DeviceCtx& g);
+  bool inited_ = false;
+  bool initialized_ = false;
+  std::deque<long> queue_;
+  long tag_ = 0;
+};
+
+void check(cudaError_t e, const char* what);
+
+}  // namespace ppcb

@@ -1,0 +1,830 @@
+// Photon propagation kernels for sm_100a.
+//
+// Physics restated from the reference kernel gpu/pro.cu:287-904 (phase 1: source
+// sampling :334-477, phase 2: stepping :486-889); the helpers cite their lines below.
+// B200-specific structure (not in the reference):
+//   * one persistent launch; phase 1 is fused into phase 2 -- a thread samples a new
+//     photon only when its previous one is absorbed, so the 48-byte per-photon phase-1
+//     record never round-trips through HBM;
+//   * photon indices are handed out by one warp-aggregated atomic per refill (one
+//     global counter, 64-bit, so a launch may cover more than 2^32 photons), or
+//     statically (photon i on thread i mod T) in deterministic mode;
+//   * the photon -> bunch map is a binary search over an exclusive prefix sum, so a
+//     launch may hold thousands of bunches/events;
+//   * the small tables (per-layer anisotropy/BFR, strings, cell index, tilt radii) sit
+//     in shared memory; the per-wavelength ice table, tilt maps and DOMs are read
+//     through the read-only cache from HBM (they are L2-resident: < 1 MB);
+//   * hits are appended with one atomic per coalesced group of hitting lanes;
+//   * the index helpers (tilt shift, layer, cell range, DOM window) use explicit
+//     round-to-nearest operations without contraction, so for identical positions they
+//     are bit-identical to the IEEE CPU restatement; the rest of the physics uses the
+//     same fast-math intrinsics as the reference's GPU build (--use_fast_math).
+#include <cooperative_groups.h>
+
+#include "propagate.cuh"
+#include "tilt.h"
+
+namespace cg = cooperative_groups;
+
+namespace ppcb {
+
+#define XXX PPCB_XXX
+#define FPI PPCB_FPI
+#define OMR PPCB_OMR
+#define WNUM PPCB_WNUM
+
+__device__ __constant__ float kFcv = PPCB_FPI / 180.f;
+
+struct SmemTables {
+  ppcb_aniz az[PPCB_MAXLYS];
+  ppcb_line sc[PPCB_NSTR];
+  float lr[PPCB_LMAX];
+  uint16_t ls[PPCB_NSTR];
+  uint16_t is[PPCB_CX * PPCB_CY];
+  int8_t mcol[PPCB_CTX * PPCB_CTY];
+};
+
+// ---------------------------------------------------------------- IEEE helpers
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ int imin(int a, int b) { return b < a ? b : a; }
+__device__ __forceinline__ int imax(int a, int b) { return a < b ? b : a; }
+
+struct Rng {
+  uint32_t x, y, a;
+};
+
+// gpu/pro.cu:47-57: 64-bit multiply-with-carry, (0,1]
+__device__ __forceinline__ float xrnd(Rng& s) {
+  unsigned long long sda = (unsigned long long)s.a * s.x + s.y;
+  s.x = (uint32_t)sda;
+  s.y = (uint32_t)(sda >> 32);
+  return 2.f - __uint_as_float((s.x >> 9) | 0x3f800000u);
+}
+
+// gpu/pro.cu:59-85
+__device__ float mrnd(float k, Rng& s) {
+  float x;
+  if (k < 1) {
+    float c = 1 / k;
+    float d = (1 - k) * powf(k, 1 / (c - 1));
+    float z, e;
+    do {
+      z = -logf(xrnd(s));
+      e = -logf(xrnd(s));
+      x = powf(z, c);
+    } while (z + e < d + x);
+  } else {
+    float b = k - logf(4.0f);
+    float l = sqrtf(2 * k - 1);
+    float c = 1 + logf(4.5f);
+    float u, v, y, z, r;
+    do {
+      u = xrnd(s);
+      v = xrnd(s);
+      y = -logf(1 / v - 1) / l;
+      x = k * expf(y);
+      z = u * v * v;
+      r = b + (k + l) * y - x;
+    } while (r < 4.5f * z - c && r < logf(z));
+  }
+  return x;
+}
+
+// gpu/pro.cu:87-95
+__device__ __forceinline__ float grnd(Rng& s) {
+  float a = sqrtf(-2 * logf(xrnd(s)));
+  return a * sinf(2 * FPI * xrnd(s));
+}
+
+__device__ __forceinline__ float2 grnd2(Rng& s) {
+  float r = sqrtf(-2 * logf(xrnd(s)));
+  float2 p;
+  sincosf(2 * FPI * xrnd(s), &p.y, &p.x);
+  p.x *= r;
+  p.y *= r;
+  return p;
+}
+
+__device__ __forceinline__ void swp(float& a, float& b) { float t = a; a = b; b = t; }
+
+// gpu/pro.cu:111-153: rotate n by polar angle (cs = 1-cos, si = sin), uniform azimuth
+__device__ __forceinline__ void rotate(float cs, float si, float4& n, Rng& s) {
+  float3 p1, p2;
+  int i = 0;
+  {
+    float3 r;
+    r.x = n.x * n.x; r.y = n.y * n.y; r.z = n.z * n.z;
+    if (r.y > r.z) {
+      if (r.y > r.x) { swp(n.x, n.y); swp(r.x, r.y); i = 1; }
+    } else {
+      if (r.z > r.x) { swp(n.x, n.z); swp(r.x, r.z); i = 2; }
+    }
+    r.y = rsqrtf(r.x + r.y); p1.x = -n.y * r.y; p1.y = n.x * r.y; p1.z = 0;
+    r.z = rsqrtf(r.x + r.z); p2.x = -n.z * r.z; p2.y = 0; p2.z = n.x * r.z;
+  }
+  {
+    float3 q1;
+    q1.x = p1.x - p2.x; q1.y = p1.y - p2.y; q1.z = p1.z - p2.z;
+    p2.x += p1.x; p2.y += p1.y; p2.z += p1.z;
+    float w = rsqrtf(q1.x * q1.x + q1.y * q1.y + q1.z * q1.z);
+    p1.x = q1.x * w; p1.y = q1.y * w; p1.z = q1.z * w;
+    w = rsqrtf(p2.x * p2.x + p2.y * p2.y + p2.z * p2.z);
+    p2.x *= w; p2.y *= w; p2.z *= w;
+  }
+  {
+    float2 p;
+    float xi = 2 * FPI * xrnd(s);
+    sincosf(xi, &p.y, &p.x);
+    n.x -= cs * n.x - si * (p.x * p1.x + p.y * p2.x);
+    n.y -= cs * n.y - si * (p.x * p1.y + p.y * p2.y);
+    n.z -= cs * n.z - si * (p.x * p1.z + p.y * p2.z);
+    float r = rsqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+    n.x *= r; n.y *= r; n.z *= r;
+    if (i == 1) swp(n.x, n.y);
+    else if (i == 2) swp(n.x, n.z);
+  }
+}
+
+__device__ __forceinline__ void normalize3(float4& n) {
+  float r = rsqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+  n.x *= r; n.y *= r; n.z *= r;
+}
+
+// ---------------------------------------------------------------- index helpers
+// tilt tables as seen by the kernel: radii and map columns in shared memory, the
+// depth maps through the read-only cache
+struct DevTilt {
+  const SmemTables& S;
+  const ppcb_params& d;
+  const float2* __restrict__ lpg;
+  __device__ __forceinline__ float lr(int i) const { return S.lr[i]; }
+  __device__ __forceinline__ int mcol(int x, int y) const {
+    return x >= 0 && x < d.mnum[0] && y >= 0 && y < d.mnum[1] ? S.mcol[x * PPCB_CTY + y] : -1;
+  }
+  __device__ __forceinline__ float2 lp(int i, int k) const { return __ldg(&lpg[i * PPCB_LYRS + k]); }
+};
+
+__device__ __forceinline__ float zshift(const ppcb_params& d, const SmemTables& S, const float2* __restrict__ lp,
+                                        float rx, float ry, float rz, float& dz) {
+  DevTilt t{S, d, lp};
+  return zshift_t(d, t, rx, ry, rz, dz);
+}
+
+// gpu/pro.cu:507-515: tilt-corrected depth in layer units and the current layer.
+__device__ __forceinline__ int layer_of(const ppcb_params& d, float rz, float zs, float& z) {
+  z = fm(fs(fs(rz, zs), d.hmin), d.rdh);
+  return imin(imax(__float2int_rn(z), 0), d.size - 1);
+}
+
+// gpu/pro.cu:580-594: range of search cells covered by a segment (plus margin rx).
+__device__ __forceinline__ void cell_range(const ppcb_params& d, float rx0, float ry0, float rx1, float ry1,
+                                           int& xlx, int& xhx, int& xly, int& xhy) {
+  float pix = fa(fm(d.cb[0][0], rx0), fm(d.cb[1][0], ry0));
+  float piy = fa(fm(d.cb[0][1], rx0), fm(d.cb[1][1], ry0));
+  float pfx = fa(fm(d.cb[0][0], rx1), fm(d.cb[1][0], ry1));
+  float pfy = fa(fm(d.cb[0][1], rx1), fm(d.cb[1][1], ry1));
+  float lx = fs(fminf(pix, pfx), d.rx), hx = fa(fmaxf(pix, pfx), d.rx);
+  float ly = fs(fminf(piy, pfy), d.rx), hy = fa(fmaxf(piy, pfy), d.rx);
+  xlx = imin(imax(__float2int_rn(fm(fs(lx, d.cl[0]), d.crst[0])), 0), d.cn[0]);
+  xhx = imax(imin(__float2int_rn(fm(fs(hx, d.cl[0]), d.crst[0])), d.cn[0] - 1), -1);
+  xly = imin(imax(__float2int_rn(fm(fs(ly, d.cl[1]), d.crst[1])), 0), d.cn[1]);
+  xhy = imax(imin(__float2int_rn(fm(fs(hy, d.cl[1]), d.crst[1])), d.cn[1] - 1), -1);
+}
+
+// gpu/pro.cu:623-626: DOMs of one string whose depth window overlaps [zl, zh].
+__device__ __forceinline__ void dom_window(const ppcb_line& s, float zl, float zh, int& n1, int& n2) {
+  const int omin = 0, omax = s.max;
+  n1 = s.n - omin + imin(omax + 1, imax(omin, __float2int_ru(fs((float)omin, fm(fs(fs(zh, s.dl), s.h), s.d)))));
+  n2 = s.n - omin + imax(omin - 1, imin(omax, __float2int_rd(fs((float)omin, fm(fs(fs(zl, s.dh), s.h), s.d)))));
+}
+
+// ---------------------------------------------------------------- photon state
+struct Photon {
+  float4 r, n;     // position/time, direction/(1/group velocity)
+  float TOT, SCA;  // remaining absorption / scattering optical depths
+  int wl;          // wavelength bin
+  uint32_t niw;    // segment id
+  int old;         // DOM excluded from the search (last hit / flasher)
+  int ofla;        // DOM that absorbs without registering (flasher), or <-1 veto code
+  int om0;         // flasher DOM on the first step, -1 afterwards
+  uint32_t steps;
+};
+
+__device__ __forceinline__ int find_bunch(const KArgs& a, uint64_t i, int hint) {
+  // exclusive prefix sums: bunch k holds photons [bstart[k], bstart[k+1])
+  if (hint >= 0 && hint < a.nb && __ldg(&a.bstart[hint]) <= i && i < __ldg(&a.bstart[hint + 1])) return hint;
+  int lo = 0, hi = a.nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&a.bstart[mid]) <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// gpu/pro.cu:335-476: phase-1 source sampling of one photon of bunch p.
+__device__ __forceinline__ void generate(const KArgs& a, const ppcb_bunch& p, Rng& s, Photon& ph) {
+  const ppcb_params& e = a.p;
+  float4 r, n;
+  int j = imin(__float2int_rd(WNUM * xrnd(s)), WNUM - 1);
+  const ppcb_wmeta w = a.wmeta[j];
+  n.w = w.ocm;
+  r = make_float4(p.r[0], p.r[1], p.r[2], p.r[3]);
+  n.x = p.n[0]; n.y = p.n[1]; n.z = p.n[2];
+  float l = p.n[3];
+  int fla, ofla;
+  if (p.type > 0) {
+    const float ka = p.u.l.ka, up = p.u.l.up, fldr = p.u.l.fldr;
+    fla = p.u.l.fla; ofla = p.u.l.ofla;
+    if (l == 0) {  // N-fold / cylindrical LED pattern
+      float xi = xrnd(s);
+      if (fldr < 0) xi *= 2 * FPI;
+      else {
+        int rr = __float2int_rd(fldr / 360) + 1;
+        int ss = __float2int_rd(xi * rr);
+        xi = (fldr + ss * 360 / rr) * kFcv;
+      }
+      sincosf(xi, &r.y, &r.x);
+      sincosf(up, &n.z, &xi);
+      n.x = xi * r.x; n.y = xi * r.y;
+    }
+    if (ka != 0) {
+      float xi;
+      if (ka > 999.f) {  // lab-measured beam profile
+        xi = xrnd(s);
+        float s1 = 0.0191329f, s2 = 0.0686944f, C1 = 0.583583f, C2 = 0.967762f;
+        switch (p.type) {
+          case 1: s1 = 0.0196242f; s2 = 0.0750278f; C1 = 0.606833f; C2 = 0.960863f; break;
+          case 2: s1 = 0.0185603f; s2 = 0.0624481f; C1 = 0.553192f; C2 = 0.974129f; break;
+        }
+        xi = xi < C1 ? s1 * fabsf(grnd(s)) : xi < C2 ? -s2 * logf(xrnd(s)) : 2.f;
+        if (xi >= 2.f) xi = 2 * (1 - sqrtf(xrnd(s)));
+      } else if (ka > 0) xi = fminf(-ka * logf(1 - (1 - xrnd(s)) * (1 - expf(-2 / ka))), 2.f);
+      else if (ka == -1) xi = 2 * (1 - xrnd(s));
+      else xi = 2 * (1 - sqrtf(xrnd(s)));
+      rotate(xi, sqrtf(xi * (2 - xi)), n, s);
+    }
+    if (ka > 999.f) {  // start on the DOM surface; harness and cable vetoes
+      const float FLZ = 0.07735f, FLR = 0.119f - 0.008f, FLB = 0.03396f;
+      if (l == 0) { r.x *= FLR; r.y *= FLR; r.z = FLZ; r.w = 0; }
+      float b = r.x * n.x + r.y * n.y + r.z * n.z;
+      float c = FLZ * FLZ + FLR * FLR - OMR * OMR;
+      float t = sqrtf(b * b - c) - b;
+      r.x += t * n.x; r.y += t * n.y; r.z += t * n.z; r.w += t * e.ocv;
+      if (fabsf(r.z) < FLB) ofla = -2;
+      else if (l == 0 && r.z < 0 && xrnd(s) < 0.9f) ofla = -3;
+      if (ka > 1050.f) {
+        const float rc = 0.023f;
+        const float dc = OMR + rc;
+        float ph = (ka - 1080.f) * kFcv;
+        float drx = r.x - dc * cosf(ph);
+        float dry = r.y - dc * sinf(ph);
+        float aa = n.x * n.x + n.y * n.y;
+        if (aa > 0) {
+          float bb = n.x * drx + n.y * dry;
+          float cc = drx * drx + dry * dry - rc * rc;
+          float D = bb * bb - aa * cc;
+          if (D >= 0) {
+            float h1 = (-bb + sqrtf(D)) / aa;
+            if (h1 > 0) ofla = -4;
+          }
+        }
+      }
+      if (l == 0) { r.x += p.r[0]; r.y += p.r[1]; r.z += p.r[2]; r.w += p.r[3]; }
+      else {
+        const ppcb_dom dom = a.oms[fla];
+        r.x += dom.r[0]; r.y += dom.r[1]; r.z += dom.r[2]; r.w += p.r[3];
+      }
+    } else if (fla >= 0) {
+      const float t = OMR;
+      r.x = t * n.x; r.y = t * n.y; r.z = t * n.z; r.w = t * e.ocv;
+      r.x += p.r[0]; r.y += p.r[1]; r.z += p.r[2]; r.w += p.r[3];
+    } else {
+      r = make_float4(p.r[0], p.r[1], p.r[2], p.r[3]);
+    }
+  } else {
+    const float pa = p.u.p.a, pb = p.u.p.b, beta0 = p.u.p.beta, tau = p.u.p.tau;
+    fla = -1; ofla = -1;
+    if (l > 0) l *= xrnd(s);
+    else l = pb * mrnd(pa, s);
+    if (l > 0) {
+      r.x += l * n.x; r.y += l * n.y; r.z += l * n.z;
+      r.w += l * e.ocv / beta0;
+    }
+    if (tau > 0) {  // isotropic delayed emission
+      r.w -= tau * logf(xrnd(s));
+      float xi = 1 - xrnd(s);
+      rotate(xi, sqrtf(xi * (2 - xi)), n, s);
+    } else {
+      float cs = w.coschr, si = w.sinchr;
+      if (p.f < xrnd(s)) {  // cascade secondary directions
+        const float aa = 0.39f, bb = 2.61f;
+        const float I = 1 - expf(-bb * exp2f(aa));
+        float xi = fminf(powf(-logf(1 - xrnd(s) * I) / bb, 1 / aa), 2.f);
+        rotate(xi, sqrtf(xi * (2 - xi)), n, s);
+      } else {
+        float beta = beta0;
+        if (p.type < 0) {  // muon slowing down near its end point
+          const float ar = 0.26f * 0.9216f / 0.105658389f;
+          float dx = ar * (p.n[3] - l);
+          beta = sqrtf(dx * (2 + dx)) / (1 + dx);
+          if (beta >= cs) r.w -= e.ocv * (sqrtf(dx * dx + 1) - asinhf(1 / dx) - dx) / ar;
+        }
+        if (beta < 1) {
+          float xi = cs / beta;
+          if (xi <= 1) {
+            float sx = sqrtf(1 - xi * xi);
+            if (p.type < 0 && sx < xrnd(s) * si) ofla = -3;
+            cs = xi; si = sx;
+          } else ofla = -2;
+        }
+      }
+      rotate(1 - cs, si, n, s);  // Cherenkov cone
+    }
+  }
+  ph.r = r; ph.n = n;
+  ph.wl = j; ph.niw = p.q; ph.om0 = fla; ph.ofla = ofla;
+}
+
+__device__ __forceinline__ float2 ice(const float2* __restrict__ t, int J) { return __ldg(&t[J]); }
+
+__device__ __forceinline__ void emit_hit(const KArgs& a, const ppcb_hit& h) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(&a.ctrl->hidx, (unsigned long long)g.size());
+  base = g.shfl(base, 0) + g.thread_rank();
+  if (base < a.hcap) {
+    uint4* dst = reinterpret_cast<uint4*>(&a.hits[base]);
+    const uint4* src = reinterpret_cast<const uint4*>(&h);
+    dst[0] = src[0];
+    dst[1] = src[1];
+  }
+}
+
+// gpu/pro.cu:499-888: one propagation step (one scattering segment).  Returns with
+// ph.TOT == 0 once the photon is absorbed or registered.
+__device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon& ph, Rng& s,
+                                     unsigned int& nan_steps) {
+  const ppcb_params& e = a.p;
+  const float2* __restrict__ wz = a.absca + (size_t)ph.wl * e.size;
+  float4 r = ph.r, n = ph.n;
+  float TOT = ph.TOT, SCA = ph.SCA;
+  int om = ph.om0;
+  float sqd = 0;
+  if (SCA == 0) { SCA = -logf(xrnd(s)); ph.old = om; }
+  const int old = ph.old;
+  float sca, tot;
+  int sign = n.z < 0 ? -1 : 1;
+  float anz = sign * n.z;
+  float edh = e.dh;
+  float zs = zshift(e, S, a.lp, r.x, r.y, r.z, edh);
+  float z;
+  int I = layer_of(e, r.z, zs, z);
+  int J;
+  float nr = 1.f;
+  {
+    if (TOT > 0) {  // absorption anisotropy, gpu/pro.cu:517-544
+      float n1 = e.azx * n.x + e.azy * n.y;
+      float n2 = -e.azy * n.x + e.azx * n.y;
+      float n3 = n.z;
+      if (e.fr != 0) {
+        float k1 = S.az[I].k1, k2 = S.az[I].k2;
+        float kz = 1 / (k1 * k2);
+        float s1 = n1 * n1, l1 = k1 * k1;
+        float s2 = n2 * n2, l2 = k2 * k2;
+        float s3 = n3 * n3, l3 = kz * kz;
+        float B2 = nr / l1 + nr / l2 + nr / l3;
+        float nB = s1 / l1 + s2 / l2 + s3 / l3;
+        float An = s1 * l1 + s2 * l2 + s3 * l3;
+        nr = powf((B2 - nB) * An / 2, e.fr);
+      }
+      n1 *= e.k1; n2 *= e.k2; n3 *= e.kz;
+      nr *= rsqrtf(n1 * n1 + n2 * n2 + n3 * n3);
+      TOT /= nr;
+    }
+    float ahx = edh * (0.5f - sign * (z - I));
+    J = I;  // layer stepping, gpu/pro.cu:548-571
+    sca = 0; tot = 0;
+    float ais = SCA, aia = TOT;
+    float2 c = ice(wz, J);
+    while (true) {
+      float dsca = ais / c.y, dtot = aia / c.x;
+      float dist = fminf(dsca, dtot) * anz;
+      if ((sign < 0 ? J > 0 : J < e.size - 1) && dist > ahx) {
+        float del = ahx / anz;
+        sca += del; tot += del;
+        ais -= c.y * del; aia -= c.x * del;
+        ahx = edh;
+        J += sign;
+        c = ice(wz, J);
+      } else {
+        sca += dsca; tot += dtot;
+        break;
+      }
+    }
+    if (sca < 0) sca = 0;
+    if (tot < 0) tot = 0;
+    if (tot < sca) { sca = tot; tot = 0; }
+    else tot = (tot - sca) * c.x;
+  }
+
+  om = -1;
+  float del = sca;
+  float hi = sca, hf = 0;
+  {  // DOM search, gpu/pro.cu:577-672
+    int xlx, xhx, xly, xhy;
+    cell_range(e, r.x, r.y, fa(r.x, fm(sca, n.x)), fa(r.y, fm(sca, n.y)), xlx, xhx, xly, xhy);
+    const bool hole_on = e.hr > 0 && (e.hifl == 0 || (e.hifl < 0 && r.w < -e.hifl) || (e.hifl > 0 && r.w > e.hifl));
+    for (int i = xlx, j = xly; i <= xhx && j <= xhy; (++j <= xhy) ? 0 : (j = xly, i++)) {
+      for (unsigned int k = S.is[i * PPCB_CY + j]; k != 0x8000;) {
+        unsigned int m = S.ls[k];
+        const ppcb_line& sl = S.sc[m & 0x7fff];
+        k = (m & 0x8000) ? 0x8000 : k + 1;
+        float b = 0, c = 0, dr;
+        dr = sl.x - r.x; b += n.x * dr; c += dr * dr;
+        dr = sl.y - r.y; b += n.y * dr; c += dr * dr;
+        float np = 1 - n.z * n.z;
+        float D = b * b - (c - sl.r * sl.r) * np;
+        if (D >= 0) {
+          D = sqrtf(D);
+          float h1 = b - D, h2 = b + D;
+          if (h2 >= 0 && h1 <= sca * np) {
+            if (np > XXX) {
+              h1 /= np; h2 /= np;
+              if (h1 < 0) h1 = 0;
+              if (h2 > sca) h2 = sca;
+            } else { h1 = 0; h2 = sca; }
+            h1 = r.z + n.z * h1; h2 = r.z + n.z * h2;
+            float zl, zh;
+            if (n.z > 0) { zl = h1; zh = h2; }
+            else { zl = h2; zh = h1; }
+            int n1, n2;
+            dom_window(sl, zl, zh, n1, n2);
+            for (int l = n1; l <= n2; l++) if (l != old) {
+              const ppcb_dom dom = a.oms[l];
+              float aa = 0, bb = 0, cc = 0, dd;
+              float fq = dom.F > 0 ? (1 / dom.F) * (1 / dom.F) : 0;
+              dd = dom.r[0] - r.x; aa += n.x * n.x; bb += n.x * dd; cc += dd * dd;
+              dd = dom.r[1] - r.y; aa += n.y * n.y; bb += n.y * dd; cc += dd * dd;
+              dd = dom.r[2] - r.z; aa += fq * n.z * n.z; bb += fq * n.z * dd; cc += fq * dd * dd;
+              if (aa > 0) {
+                bb /= aa;
+                float xR = (l == ph.ofla ? 1 : e.xR);
+                float DD = bb * bb - (cc - (xR * dom.R) * (xR * dom.R)) / aa;
+                if (DD >= 0) {
+                  sqd = sqrtf(DD);
+                  float h = bb - sqd;
+                  if (dom.F > 0 || fabsf(dd - n.z * h) < -xR * dom.F * dom.R) {
+                    sqd /= xR; h = bb - sqd;
+                    if (h > 0 && h <= del) { om = l; del = h; }
+                  }
+                }
+              }
+            }
+          }
+        }
+        if (hole_on) {  // hole-ice column around the string
+          float DH = b * b - (c - e.hr2) * np;
+          if (DH > 0) {
+            DH = sqrtf(DH);
+            float h1 = b - DH, h2 = b + DH;
+            if (h2 >= 0 && h1 <= sca * np) {
+              if (np > XXX) {
+                h1 /= np; h2 /= np;
+                if (h1 < 0) h1 = 0;
+                if (h2 > sca) h2 = sca;
+              } else { h1 = 0; h2 = sca; }
+              if (h1 < hi && h2 > sqrtf(XXX) * e.hr) { hi = h1; hf = h2; }
+            }
+          }
+        }
+      }
+    }
+  }
+
+  float fin = fminf(del, hi);
+  bool hole = fin < sca;
+  if (hole) {  // truncated step: overburden by layers, hole ice, gpu/pro.cu:677-717
+    {
+      float xs = 0, xa = 0;
+      float y = z + n.z * fin / edh;
+      J = imin(imax(__float2int_rn(y), 0), e.size - 1);
+      if (I == J) { float2 c = ice(wz, I); xs = fin * c.y; xa = fin * c.x; }
+      else {
+        float h = 0.5f - sign * (z - I);
+        float g = 0.5f + sign * (y - J);
+        float2 ci = ice(wz, I), cj = ice(wz, J);
+        xs = h * ci.y + g * cj.y;
+        xa = h * ci.x + g * cj.x;
+        for (int i = I + sign; i != J; i += sign) { float2 c = ice(wz, i); xs += c.y; xa += c.x; }
+        float f = edh / anz;
+        xs *= f; xa *= f;
+      }
+      if (xs < 0) xs = 0;
+      if (xa < 0) xa = 0;
+      SCA -= xs; TOT -= xa;
+    }
+    TOT *= nr;
+    if (hi < del) {
+      float fin2 = fminf(hi + fminf(SCA / e.hs, TOT / e.ha), hf);
+      if (om != -1) { if (fin2 < del) { del = fin2; om = -1; } }
+      else {
+        if (fin2 < del) del = fin2;
+        else del = fminf(fin2, sca);
+      }
+      fin2 = del - hi;
+      SCA -= fin2 * e.hs; TOT -= fin2 * e.ha;
+    }
+  } else { SCA = 0; TOT = tot * nr; }
+
+  r.x += del * n.x; r.y += del * n.y; r.z += del * n.z; r.w += del * n.w;
+
+  if (!isfinite(TOT) || !isfinite(SCA)) {  // gpu/pro.cu:728
+    unsigned int k = atomicAdd(&a.ctrl->nan_steps, 1u);
+    if (k < 4) { unsigned int sm; asm volatile("mov.u32 %0, %%smid;" : "=r"(sm)); a.ctrl->bad_sm[k] = sm; }
+    TOT = 0; om = -1;
+    nan_steps++;
+  }
+
+  if (om != -1) {  // DOM hit, gpu/pro.cu:731-753
+    if (om == ph.ofla) TOT = 0;
+    else {
+      ppcb_hit h;
+      h.i = om; h.t = r.w; h.n = ph.niw; h.z = a.wmeta[ph.wl].wvl;
+      h.pth = acosf(n.z); h.pph = atan2f(n.y, n.x);
+      sqd *= e.xR - 1;
+      const ppcb_dom dom = a.oms[om];
+      float dx = dom.r[0] - r.x + sqd * n.x;
+      float dy = dom.r[1] - r.y + sqd * n.y;
+      float dz = dom.r[2] - r.z + sqd * n.z;
+      h.dth = acosf(fminf(fmaxf(dz / (e.xR * dom.R * dom.F), -1.f), 1.f));
+      h.dph = atan2f(dy, dx);
+      emit_hit(a, h);
+      if (e.xR == 1) TOT = 0;
+      else ph.old = om;
+    }
+  }
+
+  if (TOT < XXX) TOT = 0;
+  else {
+    if (e.sum > 0 && fin > 0) {  // birefringence diffusion, gpu/pro.cu:757-836
+      float ra, rb;
+      if (I == J) { ra = fin * S.az[I].ra; rb = fin * S.az[I].rb; }
+      else {
+        float y = z + n.z * fin / edh;
+        float h = 0.5f - sign * (z - I);
+        float g = 0.5f + sign * (y - J);
+        ra = h * S.az[I].ra + g * S.az[J].ra;
+        rb = h * S.az[I].rb + g * S.az[J].rb;
+        for (int i = I + sign; i != J; i += sign) { ra += S.az[i].ra; rb += S.az[i].rb; }
+        float f = edh / anz;
+        ra *= f; rb *= f;
+      }
+      if (ra < 0) ra = 0;
+      if (rb < 0) rb = 0;
+      float dot = e.azx * n.x + e.azy * n.y;
+      float sdt = sqrtf(1 - dot * dot);
+      float cdt = fabsf(dot);
+      const float* bf = e.bfr;
+      float sx = sqrtf(ra) * fmaxf(0.f, bf[0] * expf(-bf[1] * powf(atanf(bf[3] * sdt), bf[2])));
+      float sy = sqrtf(ra) * fmaxf(0.f, bf[4] * expf(-bf[5] * powf(atanf(bf[7] * sdt), bf[6])));
+      float mx = rb * fmaxf(0.f, bf[8] * atanf(bf[11] * sdt * cdt) * expf(-bf[9] * sdt + bf[10] * cdt));
+      float qx = e.azx - dot * n.x, qy = e.azy - dot * n.y, qz = -dot * n.z;
+      if (dot < 0) { qx = -qx; qy = -qy; qz = -qz; }
+      float qn = qx * qx + qy * qy + qz * qz;
+      if (qn > 0) {
+        float f = rsqrtf(qn);
+        qx *= f; qy *= f; qz *= f;
+      } else { qx = 0; qy = 0; qz = 1; }
+      float px = n.y * qz - n.z * qy, py = n.z * qx - n.x * qz, pz = n.x * qy - n.y * qx;
+      float2 rnd = grnd2(s);
+      float dnx = sx * rnd.x + mx;
+      float dny = sy * rnd.y;
+      if (del <= hi) {  // curved path within the segment
+        rnd = grnd2(s);
+        float vnx = dnx + sx * rnd.x * rsqrtf(3.f);
+        float vny = dny + sy * rnd.y * rsqrtf(3.f);
+        vnx /= 2; vny /= 2;
+        float den = vnx * vnx + vny * vny;
+        float dnz = -den;
+        den = 2 / (1 + den);
+        vnx *= den; vny *= den; dnz *= den;
+        float4 m;
+        m.x = n.x + qx * vnx + px * vny + n.x * dnz;
+        m.y = n.y + qy * vnx + py * vny + n.y * dnz;
+        m.z = n.z + qz * vnx + pz * vny + n.z * dnz;
+        normalize3(m);
+        del -= fin / 2;
+        r.x += del * (m.x - n.x);
+        r.y += del * (m.y - n.y);
+        r.z += del * (m.z - n.z);
+      }
+      dnx /= 2; dny /= 2;
+      float den = dnx * dnx + dny * dny;
+      float dnz = -den;
+      den = 2 / (1 + den);
+      dnx *= den; dny *= den; dnz *= den;
+      n.x += qx * dnx + px * dny + n.x * dnz;
+      n.y += qy * dnx + py * dny + n.y * dnz;
+      n.z += qz * dnx + pz * dny + n.z * dnz;
+      normalize3(n);
+    }
+    if (SCA < XXX) {  // scattering, gpu/pro.cu:838-887
+      SCA = 0;
+      float sf, g, gr;
+      if (hole) { sf = e.SF; g = e.G; gr = e.GR; }
+      else { sf = e.sf; g = e.g; gr = e.gr; }
+      float xi = xrnd(s);
+      if (xi > sf) {
+        xi = (1 - xi) / (1 - sf);
+        xi = 2 * xi - 1;
+        if (g != 0) {
+          float ga = (1 - g * g) / (1 + g * xi);
+          xi = (ga * ga - (1 - g) * (1 - g)) / (2 * g);
+        }
+      } else {
+        xi /= sf;
+        xi = 2 * (1 - powf(xi, gr));
+      }
+      if (xi < 0) xi = 0;
+      else if (xi > 2) xi = 2;
+      const float k1 = S.az[J].k1, k2 = S.az[J].k2;
+      const float okz = k1 * k2;
+      if (!hole) {  // stretch into the anisotropic frame
+        float n1 = (e.azx * n.x + e.azy * n.y) * k1;
+        float n2 = (-e.azy * n.x + e.azx * n.y) * k2;
+        n.x = n1 * e.azx - n2 * e.azy;
+        n.y = n1 * e.azy + n2 * e.azx;
+        n.z /= okz;
+        normalize3(n);
+      }
+      rotate(xi, sqrtf(xi * (2 - xi)), n, s);
+      if (!hole) {
+        float n1 = (e.azx * n.x + e.azy * n.y) / k1;
+        float n2 = (-e.azy * n.x + e.azx * n.y) / k2;
+        n.x = n1 * e.azx - n2 * e.azy;
+        n.y = n1 * e.azy + n2 * e.azx;
+        n.z *= okz;
+        normalize3(n);
+      }
+    }
+  }
+  ph.r = r; ph.n = n; ph.TOT = TOT; ph.SCA = SCA; ph.om0 = -1;
+}
+
+__device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
+  const int nt = blockDim.x, t = threadIdx.x;
+  for (int i = t; i < a.p.size; i += nt) S.az[i] = a.az[i];
+  for (int i = t; i < a.p.nstr; i += nt) S.sc[i] = a.sc[i];
+  for (int i = t; i < PPCB_LMAX; i += nt) S.lr[i] = a.lr[i];
+  for (int i = t; i < PPCB_NSTR; i += nt) S.ls[i] = a.ls[i];
+  for (int i = t; i < PPCB_CX * PPCB_CY; i += nt) S.is[i] = a.is[i];
+  for (int i = t; i < PPCB_CTX * PPCB_CTY; i += nt) S.mcol[i] = a.mcol[i];
+  __syncthreads();
+}
+
+#define PPCB_BLOCK 256
+#define PPCB_MINB 3
+
+__global__ void __launch_bounds__(PPCB_BLOCK, PPCB_MINB) k_propagate(const __grid_constant__ KArgs a) {
+  __shared__ SmemTables S;
+  load_tables(a, S);
+  const uint32_t T = gridDim.x * blockDim.x;
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned int lane = threadIdx.x & 31;
+  Rng s;
+  {
+    uint64_t st = a.rs[gt];
+    s.x = (uint32_t)st; s.y = (uint32_t)(st >> 32); s.a = a.rm[gt];
+  }
+  Photon ph;
+  bool alive = false;
+  uint64_t sidx = gt;
+  int hint = 0;
+  unsigned long long nsteps = 0;
+  unsigned int nan_steps = 0, capped = 0;
+  while (true) {
+    uint64_t idx = ~0ull;
+    if (a.deterministic) {
+      if (!alive) { idx = sidx; sidx += T; }
+    } else {
+      const unsigned int am = __activemask();
+      const unsigned int need = __ballot_sync(am, !alive);
+      if (need) {
+        const int leader = __ffs(need) - 1;
+        unsigned long long base = 0;
+        if ((int)lane == leader) base = atomicAdd(&a.ctrl->next, (unsigned long long)__popc(need));
+        base = __shfl_sync(am, base, leader);
+        if (!alive) idx = base + __popc(need & ((1u << lane) - 1u));
+      }
+    }
+    if (!alive) {
+      if (idx >= a.num) break;
+      hint = find_bunch(a, idx, hint);
+      const ppcb_bunch p = a.bunches[hint];
+      generate(a, p, s, ph);
+      ph.TOT = -logf(xrnd(s));
+      ph.SCA = 0;
+      ph.old = -1;
+      ph.steps = 0;
+      if (ph.ofla < -1) ph.TOT = 0;
+      alive = true;
+    }
+    step(a, S, ph, s, nan_steps);
+    ph.steps++;
+    nsteps++;
+    if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) { ph.TOT = 0; capped++; }
+    if (ph.TOT == 0) alive = false;
+  }
+  a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
+  atomicAdd(&a.ctrl->steps, nsteps);
+  if (capped) atomicAdd(&a.ctrl->capped, capped);
+}
+
+// Phase-1 only: thread t samples photon t with stream t (test entry point).
+__global__ void __launch_bounds__(PPCB_BLOCK) k_generate(const __grid_constant__ KArgs a, float4* out) {
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt >= a.num) return;
+  Rng s;
+  uint64_t st = a.rs[gt];
+  s.x = (uint32_t)st; s.y = (uint32_t)(st >> 32); s.a = a.rm[gt];
+  int b = find_bunch(a, gt, 0);
+  const ppcb_bunch p = a.bunches[b];
+  Photon ph;
+  generate(a, p, s, ph);
+  float4* o = out + 3 * (size_t)gt;
+  o[0] = ph.r;
+  o[1] = ph.n;
+  o[2] = make_float4(__int_as_float(ph.wl), __int_as_float((int)ph.niw), __int_as_float(ph.om0),
+                     __int_as_float(ph.ofla));
+  a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
+}
+
+// Index helpers at given points (test entry point).  pos[2k] = (x,y,z,t) start,
+// pos[2k+1] = (nx,ny,nz,len) direction and segment length.  Outputs per point:
+// ints  [layer, xlx, xhx, xly, xhy, n1, n2, string]   floats [zshift, dz]
+__global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos, int np, int32_t* oi, float* of) {
+  __shared__ SmemTables S;
+  load_tables(a, S);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= np) return;
+  const float4 r = pos[2 * k], n = pos[2 * k + 1];
+  float dz = a.p.dh;
+  float zs = zshift(a.p, S, a.lp, r.x, r.y, r.z, dz);
+  float z;
+  int I = layer_of(a.p, r.z, zs, z);
+  int xlx, xhx, xly, xhy;
+  cell_range(a.p, r.x, r.y, fa(r.x, fm(n.w, n.x)), fa(r.y, fm(n.w, n.y)), xlx, xhx, xly, xhy);
+  const int m = k % (a.p.nstr > 0 ? a.p.nstr : 1);
+  int n1 = 0, n2 = -1;
+  if (a.p.nstr > 0) {
+    float z1 = r.z, z2 = fa(r.z, fm(n.w, n.z));
+    dom_window(S.sc[m], fminf(z1, z2), fmaxf(z1, z2), n1, n2);
+  }
+  int32_t* o = oi + 8 * k;
+  o[0] = I; o[1] = xlx; o[2] = xhx; o[3] = xly; o[4] = xhy; o[5] = n1; o[6] = n2; o[7] = m;
+  of[2 * k] = zs;
+  of[2 * k + 1] = dz;
+}
+
+cudaError_t launch_propagate(const KArgs& a, LaunchShape sh, cudaStream_t st) {
+  if (sh.threads != PPCB_BLOCK) return cudaErrorInvalidConfiguration;
+  k_propagate<<<sh.blocks, sh.threads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_generate(const KArgs& a, LaunchShape, void* pbuf_out, cudaStream_t st) {
+  int blocks = (int)((a.num + PPCB_BLOCK - 1) / PPCB_BLOCK);
+  if (blocks == 0) return cudaSuccess;
+  k_generate<<<blocks, PPCB_BLOCK, 0, st>>>(a, (float4*)pbuf_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t* out_i, float* out_f,
+                               cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_index_probe<<<(n + 255) / 256, 256, 0, st>>>(a, pos, n, out_i, out_f);
+  return cudaGetLastError();
+}
+
+cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local) {
+  cudaFuncAttributes at;
+  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate);
+  if (e != cudaSuccess) return e;
+  *regs = at.numRegs;
+  *max_threads = at.maxThreadsPerBlock;
+  *smem = at.sharedSizeBytes;
+  *local = at.localSizeBytes;
+  return cudaSuccess;
+}
+
+int propagate_max_blocks_per_sm(int threads) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate, threads, 0) != cudaSuccess) return 0;
+  return nb;
+}
+
+}  // namespace ppcb

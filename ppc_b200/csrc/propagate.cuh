@@ -1,0 +1,55 @@
+// Kernel-facing declarations shared by the launch code and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ppcb_types.h"
+
+namespace ppcb {
+
+// Per-launch arguments, passed as a __grid_constant__ kernel parameter (constant bank).
+struct KArgs {
+  ppcb_params p;
+  // read-only tables in HBM
+  const float2* absca;       // [WNUM][size] (abs, sca)
+  const ppcb_wmeta* wmeta;   // [WNUM]
+  const float2* lp;          // [LMAX][LYRS] tilt maps
+  const ppcb_dom* oms;       // [gsize]
+  const ppcb_aniz* az;       // [size]        -> shared memory
+  const ppcb_line* sc;       // [nstr]        -> shared memory
+  const float* lr;           // [LMAX]        -> shared memory
+  const uint16_t* ls;        // [NSTR]        -> shared memory
+  const uint16_t* is;        // [CX*CY]       -> shared memory
+  const int8_t* mcol;        // [CTX*CTY]     -> shared memory
+  // work
+  const ppcb_bunch* bunches; // [nb]
+  const uint64_t* bstart;    // [nb+1] first photon index of each bunch (exclusive prefix sum)
+  int nb;
+  uint64_t num;              // photons in this launch
+  // random streams, one per thread slot
+  uint64_t* rs;              // [threads] MWC state
+  const uint32_t* rm;        // [threads] multipliers
+  // output
+  ppcb_hit* hits;
+  uint64_t hcap;
+  ppcb_ctrl* ctrl;
+  // options
+  int deterministic;         // 1: photon i runs on thread i % threads (static order)
+  uint32_t max_steps;        // 0: unlimited; else photons stopped after this many steps
+};
+
+// Launch shape chosen by the host.
+struct LaunchShape {
+  int blocks;
+  int threads;
+};
+
+// Kernel entry points (defined in propagate.cu).
+cudaError_t launch_propagate(const KArgs& a, LaunchShape s, cudaStream_t st);
+cudaError_t launch_generate(const KArgs& a, LaunchShape s, void* pbuf_out, cudaStream_t st);
+cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t* out_i, float* out_f,
+                               cudaStream_t st);
+cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local);
+int propagate_max_blocks_per_sm(int threads);
+
+}  // namespace ppcb
