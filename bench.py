@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark: photon propagation throughput (photons/s) on B200.
+
+Workload (one step, per GPU): the full-detector cascade -- 5160 DOMs on 86 strings,
+171 ice layers with a +-20 m 1-d tilt, absorption anisotropy and birefringence -- with
+1e8 propagated photons from one EM cascade (gamma longitudinal profile) at a vertex
+uniform in |x|,|y|,|z| <= 500 m and a direction uniform on the sphere, seeded per step
+and rank.  Synthetic data (ppc_b200/synth.py, configuration `full`).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:       `value` = photons / device time of the propagation launches, bunches already
+            in HBM (ppcb_propagate_device); `e2e` = the same workload through ppcb_propagate
+            with host buffers (bunch upload, launch, hit download inside the timed region).
+reference:  the reference's own CPU build (gpu/ppc.cu compiled as gpu/Makefile:10 does,
+            oracle/_ref) on every host core, same workload, bounded sample per step.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("PPCB_QUIET", "1")
+
+PHOTONS = 100_000_000
+FCV = math.pi / 180
+
+
+def _cascade_bunch(rng, photons, q=1, ppm=2450.08):
+    """EM cascade bunch with the reference's longitudinal parameters (gpu/f2k.cxx:68-79)."""
+    from ppc_b200 import types as T
+    # energy whose mean yield at xR=5 is `photons` propagated photons (gpu/f2k.cxx:68-71,
+    # :502): photons = ppm * 5.321*0.910/0.9216 * E / 25
+    E = photons * 25.0 / (ppm * 5.321 * 0.910 / 0.9216)
+    logE = math.log(max(0.105658389, E))
+    a = 2.01849 + 0.63176 * logE
+    b = 0.39652 * 0.910 / 0.9216 / 0.63207
+    v = rng.uniform(-500, 500, 3)
+    ct = rng.uniform(-1, 1)
+    ph = rng.uniform(0, 2 * math.pi)
+    st = math.sqrt(1 - ct * ct)
+    bunch = T.bunch_particle([v[0], v[1], v[2], 0.0], [st * math.cos(ph), st * math.sin(ph), ct], q, photons,
+                             -11, f=0.0, a=a, b=b)
+    return bunch, E, v
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                x = [s.strip() for s in line.split(",")]
+                if len(x) >= 9:
+                    rows.append(x)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_reference_sample(photons_per_proc, procs, seed=0):
+    """The reference CPU build (oracle/_ref/ref_harness_fm: gpu/ppc.cu + gpu/pro.cu compiled with
+    the reference's flags) propagating cascade photons in `procs` concurrent processes."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness_fm")
+    if not os.path.exists(exe):
+        return None
+    from ppc_b200 import synth
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    if not os.path.exists(os.path.join(ice, "cfg.txt")):
+        synth.write("full", ice)
+    rng = np.random.default_rng(seed)
+    ps = []
+    env = dict(os.environ, PPCTABLESDIR=ice, PPCB_QUIET="1")
+    for k in range(procs):
+        E = PHOTONS * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
+        v = rng.uniform(-500, 500, 3)
+        ct = rng.uniform(-1, 1)
+        ph = rng.uniform(0, 2 * math.pi)
+        st = math.sqrt(1 - ct * ct)
+        spec = f"cascade:{v[0]}:{v[1]}:{v[2]}:{E}:{st * math.cos(ph)}:{st * math.sin(ph)}:{ct}:11"
+        ps.append(subprocess.Popen([exe, "run", spec, str(photons_per_proc), str(seed * 1000 + k), "/tmp/ppcb_ref",
+                                    "nodump"], env=env, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+    rate, photons, secs = 0.0, 0, 0.0
+    for p in ps:
+        out, _ = p.communicate()
+        line = [l for l in out.splitlines() if l.startswith("{")][-1]
+        r = json.loads(line)
+        rate += r["photons"] / r["seconds"]
+        photons += r["photons"]
+        secs = max(secs, r["seconds"])
+    return {"value": rate, "photons": photons, "seconds": secs}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    per = args.ref_photons
+    vals = []
+    for s in range(args.warmup + args.steps):
+        r = cpu_reference_sample(per, procs, seed=s)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not built"}))
+            return
+        if s >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["value"] for r in vals])
+    line = {
+        "impl": "reference", "metric": "photons/s", "value": v, "unit": "photons/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median([r["seconds"] for r in vals]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "full-detector EM cascade, 5160 DOMs, 171 layers, 1-d tilt, anisotropy, BFR",
+                   "photons_per_step": per * procs, "l2": "n/a (host)"},
+        "cpu_baseline": {"value": v, "unit": "photons/s", "cores": procs, "kind": "reference",
+                         "sample": f"{per} photons x {procs} processes of the reference CPU build per step"},
+        "e2e": {"value": v, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from ppc_b200 import synth
+    from ppc_b200 import types as T
+    from ppc_b200.api import PPC
+
+    torch.cuda.set_device(local)
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    if not os.path.exists(os.path.join(ice, "cfg.txt")):
+        synth.write("full", ice)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+
+    c = PPC()
+    c.initialize(1.0, ice)
+    c.set_seed(1000 + rank)
+    c.choose(local)
+    c.ini()
+    info = c.info()
+    ppm = c.tables()["eff"][0]
+    rng = np.random.default_rng(17 + 1000 * rank)
+    photons = args.photons
+
+    cap = 1 << 22
+    d_hits = torch.empty((cap, 32), dtype=torch.uint8, device="cuda")
+    d_ctrl = torch.zeros(56, dtype=torch.uint8, device="cuda")
+    d_bunch = torch.empty(64, dtype=torch.uint8, device="cuda")
+    d_bstart = torch.tensor([0, photons], dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(timed):
+        b, _, _ = _cascade_bunch(rng, photons, q=1, ppm=ppm)
+        d_bunch.copy_(torch.from_numpy(b.view(np.uint8).reshape(-1)))
+        d_ctrl.zero_()
+        flush.fill_(1)  # evict L2 between timed iterations
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c.propagate_device(d_bunch.data_ptr(), d_bstart.data_ptr(), 1, photons, d_hits.data_ptr(), cap,
+                           d_ctrl.data_ptr(), stream.cuda_stream, 0)
+        e1.record(stream)
+        e1.synchronize()
+        ctrl = T.Ctrl.from_buffer_copy(d_ctrl.cpu().numpy().tobytes())
+        return e0.elapsed_time(e1), ctrl
+
+    for _ in range(args.warmup):
+        step(False)
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local) if rank == 0 else None
+    times, steps_done, hits = [], 0, 0
+    for _ in range(args.steps):
+        ms, ctrl = step(True)
+        times.append(ms)
+        steps_done += ctrl.steps
+        hits += ctrl.hidx
+    torch.cuda.synchronize()
+    clocks = clk.stop() if clk else None
+    total_ms = sum(times)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        total_ms = float(t.item())
+        td.barrier()
+
+    # end to end through the host API: bunch upload, launch, hit download
+    e2e_times, e2e_hits = [], 0
+    for k in range(args.warmup + args.steps):
+        b, _, _ = _cascade_bunch(rng, photons, q=1, ppm=ppm)
+        if dist:
+            td.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h, inf = c.propagate(b, cap=cap)
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_times.append(t1 - t0)
+            e2e_hits += len(h)
+    e2e_total = sum(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    if rank != 0:
+        return
+    value = world * photons * args.steps / (total_ms / 1000.0)
+    e2e_value = world * photons * args.steps / e2e_total
+    launch_ms = total_ms / args.steps
+    steps_per_launch = steps_done / args.steps
+    # roofline: FP32 issue.  Algorithmic FP32 operations per photon-step (measured with
+    # ncu on this kernel, thread-level FADD+FMUL+FFMA(x2), profiles/propagate_fp32_ops.md)
+    ops_per_step = args.fp32_ops_per_step
+    achieved = ops_per_step * steps_per_launch / (launch_ms / 1000.0) / 1e12
+    props = torch.cuda.get_device_properties(local)
+    sm_max = (clocks or {}).get("sm_max_mhz") or 1965.0
+    peak = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
+    h2d = 64 + 16
+    d2h = 32 * (e2e_hits / max(1, args.steps)) + 56
+    line = {
+        "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": launch_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "full-detector EM cascade, 5160 DOMs, 171 layers, 1-d tilt, anisotropy, BFR",
+                   "photons_per_step": photons, "l2": "flushed (256 MB write) before each timed step",
+                   "parallelism": f"replicas x{world}", "threads": info["threads"], "blocks": info["blocks"]},
+        "photon_steps_per_s": world * steps_done / (total_ms / 1000.0),
+        "steps_per_photon": steps_per_launch / photons,
+        "hits_per_step": hits / args.steps,
+        "gpu_launches": args.steps,
+        "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(d2h), "gpu_launches": args.steps},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"nominal FP32 issue: {props.multi_processor_count} SMs x 128 lanes x 2 flop x "
+                                    f"{sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
+                     "ops_per_photon_step": ops_per_step},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        r = cpu_reference_sample(args.ref_photons, os.cpu_count() or 1)
+        if r:
+            line["cpu_baseline"] = {"value": r["value"], "unit": "photons/s", "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"{args.ref_photons} photons x {os.cpu_count()} processes of the "
+                                              "reference CPU build (same cascade workload)"}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--photons", type=int, default=PHOTONS)
+    ap.add_argument("--ref-photons", type=int, default=200_000)
+    ap.add_argument("--fp32-ops-per-step", type=float, default=250.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as td
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -194,6 +194,28 @@ float ppco_zshift(const ppco_tables* t, const float* r, float* dz) {
   return 0;
 }
 
+/* gpu/pro.cu:580-594: search cells covered by the segment r -> r + sca*n (plus margin rx) */
+static void cell_range(const ppcb_params* e, float rx0, float ry0, float rx1, float ry1, int* xlx, int* xhx,
+                       int* xly, int* xhy) {
+  float pix = e->cb[0][0] * rx0 + e->cb[1][0] * ry0;
+  float piy = e->cb[0][1] * rx0 + e->cb[1][1] * ry0;
+  float pfx = e->cb[0][0] * rx1 + e->cb[1][0] * ry1;
+  float pfy = e->cb[0][1] * rx1 + e->cb[1][1] * ry1;
+  float lx = mnf(pix, pfx) - e->rx, hx = mxf(pix, pfx) + e->rx;
+  float ly = mnf(piy, pfy) - e->rx, hy = mxf(piy, pfy) + e->rx;
+  *xlx = mni(mxi(rn((lx - e->cl[0]) * e->crst[0]), 0), e->cn[0]);
+  *xhx = mxi(mni(rn((hx - e->cl[0]) * e->crst[0]), e->cn[0] - 1), -1);
+  *xly = mni(mxi(rn((ly - e->cl[1]) * e->crst[1]), 0), e->cn[1]);
+  *xhy = mxi(mni(rn((hy - e->cl[1]) * e->crst[1]), e->cn[1] - 1), -1);
+}
+
+/* gpu/pro.cu:623-626: DOM index window of one string for the depth range [zl, zh] */
+static void dom_window(const ppcb_line* sl, float zl, float zh, int* n1, int* n2) {
+  int omin = 0, omax = sl->max;
+  *n1 = sl->n - omin + mni(omax + 1, mxi(omin, ru(omin - (zh - sl->dl - sl->h) * sl->d)));
+  *n2 = sl->n - omin + mxi(omin - 1, mni(omax, rd(omin - (zl - sl->dh - sl->h) * sl->d)));
+}
+
 static inline float wabs(const ppco_tables* t, uint32_t w, int J) { return t->absca[((size_t)w * t->p->size + J) * 2]; }
 static inline float wsca(const ppco_tables* t, uint32_t w, int J) { return t->absca[((size_t)w * t->p->size + J) * 2 + 1]; }
 
@@ -398,18 +420,8 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
     float del = sca;
     float hi = sca, hf = 0;
     {  /* DOM search through the cell grid, gpu/pro.cu:577-672 */
-      float rix = r.x, rfx = r.x + sca * n.x;
-      float riy = r.y, rfy = r.y + sca * n.y;
-      float pix = e->cb[0][0] * rix + e->cb[1][0] * riy;
-      float piy = e->cb[0][1] * rix + e->cb[1][1] * riy;
-      float pfx = e->cb[0][0] * rfx + e->cb[1][0] * rfy;
-      float pfy = e->cb[0][1] * rfx + e->cb[1][1] * rfy;
-      rix = mnf(pix, pfx) - e->rx; rfx = mxf(pix, pfx) + e->rx;
-      riy = mnf(piy, pfy) - e->rx; rfy = mxf(piy, pfy) + e->rx;
-      int xlx = mni(mxi(rn((rix - e->cl[0]) * e->crst[0]), 0), e->cn[0]);
-      int xhx = mxi(mni(rn((rfx - e->cl[0]) * e->crst[0]), e->cn[0] - 1), -1);
-      int xly = mni(mxi(rn((riy - e->cl[1]) * e->crst[1]), 0), e->cn[1]);
-      int xhy = mxi(mni(rn((rfy - e->cl[1]) * e->crst[1]), e->cn[1] - 1), -1);
+      int xlx, xhx, xly, xhy;
+      cell_range(e, r.x, r.y, r.x + sca * n.x, r.y + sca * n.y, &xlx, &xhx, &xly, &xhy);
       for (int i = xlx, j = xly; i <= xhx && j <= xhy; (++j <= xhy) ? 0 : (j = xly, i++)) {
         for (unsigned short k = t->is[i * PPCB_CY + j]; k != 0x8000;) {
           unsigned short m = t->ls[k];
@@ -433,9 +445,8 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
               float zl, zh;
               if (n.z > 0) { zl = h1; zh = h2; }
               else { zl = h2; zh = h1; }
-              int omin = 0, omax = sl->max;
-              int n1 = sl->n - omin + mni(omax + 1, mxi(omin, ru(omin - (zh - sl->dl - sl->h) * sl->d)));
-              int n2 = sl->n - omin + mxi(omin - 1, mni(omax, rd(omin - (zl - sl->dh - sl->h) * sl->d)));
+              int n1, n2;
+              dom_window(sl, zl, zh, &n1, &n2);
               for (int l = n1; l <= n2; l++) if (l != old) {
                 const ppcb_dom* dom = &t->oms[l];
                 float a = 0, bb = 0, cc = 0, dd;
@@ -694,4 +705,28 @@ uint64_t ppco_run_fused(const ppco_tables* t, const ppcb_bunch* b, int nb, uint6
   }
   if (steps) *steps = st;
   return nh;
+}
+
+void ppco_index_probe(const ppco_tables* t, const float* pos, int n, int32_t* oi, float* of) {
+  const ppcb_params* e = t->p;
+  for (int k = 0; k < n; k++) {
+    const float* r = pos + 8 * k;
+    const float* d = r + 4;
+    float dz = e->dh;
+    float zs = ppco_zshift(t, r, &dz);
+    float z = r[2] - zs;
+    z = (z - e->hmin) * e->rdh;
+    int I = mni(mxi(rn(z), 0), e->size - 1);
+    int xlx, xhx, xly, xhy;
+    cell_range(e, r[0], r[1], r[0] + d[3] * d[0], r[1] + d[3] * d[1], &xlx, &xhx, &xly, &xhy);
+    int m = k % (e->nstr > 0 ? e->nstr : 1), n1 = 0, n2 = -1;
+    if (e->nstr > 0) {
+      float z1 = r[2], z2 = r[2] + d[3] * d[2];
+      dom_window(&t->sc[m], mnf(z1, z2), mxf(z1, z2), &n1, &n2);
+    }
+    int32_t* o = oi + 8 * k;
+    o[0] = I; o[1] = xlx; o[2] = xhx; o[3] = xly; o[4] = xhy; o[5] = n1; o[6] = n2; o[7] = m;
+    of[2 * k] = zs;
+    of[2 * k + 1] = dz;
+  }
 }

@@ -64,6 +64,10 @@ uint64_t ppco_run_reference_order(const ppco_tables* t, const ppcb_bunch* b, int
 uint64_t ppco_run_fused(const ppco_tables* t, const ppcb_bunch* b, int nb, uint64_t num, uint32_t nthr,
                         uint64_t* rs, const uint32_t* rm, ppcb_hit* hits, uint64_t cap, uint64_t* steps);
 
+/* Index helpers at points (the product's ppcb_index_probe_device counterpart):
+ * pos[8k..] = x,y,z,t, nx,ny,nz,length; out as there. */
+void ppco_index_probe(const ppco_tables* t, const float* pos, int n, int32_t* out_i, float* out_f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,7 +39,7 @@ class PPC:
     def set_seed(self, seed):
         check(lib().ppcb_set_seed(self._c, int(seed) & 0xFFFFFFFF))
 
-    def set_options(self, deterministic=False, max_steps=0, blocks_per_sm=0):
+    def set_options(self, deterministic=False, max_steps=1_000_000, blocks_per_sm=0):
         check(lib().ppcb_set_options(self._c, int(bool(deterministic)), int(max_steps), int(blocks_per_sm)))
 
     def ini(self):

@@ -74,7 +74,7 @@ def build(verbose=False):
             _run([CXX] + CXXFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
     libs = ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
-    for name, soname in (("libppcb.so", "libppcb.so"), ("libxppc.so", "xppc")):
+    for name, soname in (("libppcb.so", "libppcb.so"), ("libxppc.so", "libxppc.so")):
         out = os.path.join(LIB, name)
         if _newer(out, objs):
             _run([CXX, "-shared", "-o", out] + objs + ["-Wl,-soname," + soname] + libs)
@@ -87,6 +87,9 @@ def build(verbose=False):
     exe = os.path.join(BIN, "ppc")
     if _newer(exe, objs + cli_objs):
         _run([CXX, "-o", exe] + cli_objs + objs + libs)
+    mwc_src, mwc = os.path.join(SRC, "mwc_multipliers.c"), os.path.join(BIN, "mwc_multipliers")
+    if _newer(mwc, [mwc_src]):
+        _run(["gcc", "-O2", "-fopenmp", mwc_src, "-o", mwc])
     if verbose:
         with open(os.path.join(OBJ, "propagate.cu.ptxas.txt")) as f:
             sys.stdout.write(f.read())

@@ -72,7 +72,7 @@ class Engine {
   Config cfg;
   unsigned int sv = 0;             // seed: MWC stream start and host rand_r state
   bool deterministic = false;
-  uint32_t max_steps = 0;
+  uint32_t max_steps = 1000000;     // per-photon step cap (typical photons take 20-100 steps)
   std::vector<DeviceCtx> devs;
   uint64_t pmax = 0, pmxo = 0;     // photons / bunches per launch
   unsigned int hquo = 1;

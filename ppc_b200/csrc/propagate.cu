@@ -71,16 +71,18 @@ __device__ float mrnd(float k, Rng& s) {
     float c = 1 / k;
     float d = (1 - k) * powf(k, 1 / (c - 1));
     float z, e;
+    int guard = 0;  // bounded rejection loop (only degenerate shape parameters reach the bound)
     do {
       z = -logf(xrnd(s));
       e = -logf(xrnd(s));
       x = powf(z, c);
-    } while (z + e < d + x);
+    } while (z + e < d + x && ++guard < 100000);
   } else {
     float b = k - logf(4.0f);
     float l = sqrtf(2 * k - 1);
     float c = 1 + logf(4.5f);
     float u, v, y, z, r;
+    int guard = 0;
     do {
       u = xrnd(s);
       v = xrnd(s);
@@ -88,7 +90,7 @@ __device__ float mrnd(float k, Rng& s) {
       x = k * expf(y);
       z = u * v * v;
       r = b + (k + l) * y - x;
-    } while (r < 4.5f * z - c && r < logf(z));
+    } while (r < 4.5f * z - c && r < logf(z) && ++guard < 100000);
   }
   return x;
 }
@@ -295,7 +297,7 @@ __device__ __forceinline__ void generate(const KArgs& a, const ppcb_bunch& p, Rn
       }
       if (l == 0) { r.x += p.r[0]; r.y += p.r[1]; r.z += p.r[2]; r.w += p.r[3]; }
       else {
-        const ppcb_dom dom = a.oms[fla];
+        const ppcb_dom dom = a.oms[(unsigned)fla < (unsigned)e.gsize ? fla : 0];  // invalid input: no out-of-bounds read
         r.x += dom.r[0]; r.y += dom.r[1]; r.z += dom.r[2]; r.w += p.r[3];
       }
     } else if (fla >= 0) {
@@ -519,7 +521,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
         float2 ci = ice(wz, I), cj = ice(wz, J);
         xs = h * ci.y + g * cj.y;
         xa = h * ci.x + g * cj.x;
-        for (int i = I + sign; i != J; i += sign) { float2 c = ice(wz, i); xs += c.y; xa += c.x; }
+        for (int i = I + sign; i != J && (unsigned)i < (unsigned)e.size; i += sign) { float2 c = ice(wz, i); xs += c.y; xa += c.x; }
         float f = edh / anz;
         xs *= f; xa *= f;
       }
@@ -579,7 +581,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
         float g = 0.5f + sign * (y - J);
         ra = h * S.az[I].ra + g * S.az[J].ra;
         rb = h * S.az[I].rb + g * S.az[J].rb;
-        for (int i = I + sign; i != J; i += sign) { ra += S.az[i].ra; rb += S.az[i].rb; }
+        for (int i = I + sign; i != J && (unsigned)i < (unsigned)e.size; i += sign) { ra += S.az[i].ra; rb += S.az[i].rb; }
         float f = edh / anz;
         ra *= f; rb *= f;
       }

@@ -43,6 +43,7 @@ PPCB_HD float zshift_t(const ppcb_params& d, const Tab& t, float rx, float ry, f
     float nr = PPCB_SUB(PPCB_ADD(PPCB_MUL(d.lnx, rx), PPCB_MUL(d.lny, ry)), d.r0);
     int j = 1;
     for (; j < PPCB_LMAX; j++) if (nr < t.lr(j) || j == d.lnum - 1) break;
+    if (j >= PPCB_LMAX) j = PPCB_LMAX - 1;  // a single-map table would run off the end
     float z = PPCB_MUL(PPCB_SUB(rz, d.lmin), d.lrdz);
     int i = j - 1, k = tmin(tmax(PPCB_FLOOR_I(z), 0), d.lpts);
     const float2 pi = t.lp(i, k), pj = t.lp(j, k);

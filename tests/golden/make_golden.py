@@ -1,0 +1,87 @@
+"""Generates the golden vectors in this directory from the reference itself.
+
+Runs the reference's own code (gpu/ppc.cu + gpu/ini.cxx + gpu/pro.cu + gpu/f2k.cxx,
+compiled as its CPU build with IEEE float semantics by oracle/Makefile into
+oracle/_ref/ref_harness) on the synthetic configurations of ppc_b200/synth.py and stores:
+
+  tables_<kind>.json    sha256 of every table the reference's ini::set builds
+  zshift_<kind>.npz     tilt shift and layer thickness at fixed random points
+  run_<case>.npz        kernel-level hits, a digest of the phase-1 photon records and the
+                        final random-stream state of a fixed-seed propagation
+
+Needs /root/reference (run in the build container):  python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+os.environ.setdefault("PPCB_QUIET", "1")
+
+import oracle_util as O  # noqa: E402
+from ppc_b200 import synth  # noqa: E402
+
+TABLES = ["az", "lr", "ls", "mcol", "sc", "lp", "absca", "wmeta", "oms", "rm", "wvs", "eff"]
+
+# (case, configuration, source spec, photons, seed, environment)
+RUNS = [
+    ("small_point", "small", "point:0:0:0", 20000, 7, {"FWID": "-1", "WFLA": "405"}),
+    ("full_cascade", "full", "cascade:10:20:-300:2000:0.3:0.4:0.8660254:11", 20000, 7, {}),
+    ("full2d_flasher", "full2d", "flasher:40:30", 20000, 7, {}),
+    ("small_tilt_led", "small_tilt", "flasher:1:30", 20000, 9, {"FWID": "9.7"}),
+]
+
+
+def ice(kind):
+    path = os.path.join(ROOT, "ppc_b200", "data", "ice", kind)
+    if not os.path.exists(os.path.join(path, "cfg.txt")):
+        synth.write(kind, path)
+    return path
+
+
+def sha(b):
+    return hashlib.sha256(b).hexdigest()
+
+
+def probe_points(n, seed):
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, 0] = rng.uniform(-750, 750, n)
+    pos[:, 1] = rng.uniform(-750, 750, n)
+    pos[:, 2] = rng.uniform(-600, 600, n)
+    return pos
+
+
+def main():
+    if not O.harness_available():
+        raise SystemExit("reference harness missing: make -C oracle ref")
+    tmp = tempfile.mkdtemp()
+    for kind in ("small", "full", "full2d", "small_tilt"):
+        raw = O.harness_tables(ice(kind), tmp)
+        with open(os.path.join(HERE, f"tables_{kind}.json"), "w") as f:
+            json.dump({k: sha(raw[k]) for k in TABLES}, f, indent=1, sort_keys=True)
+    for kind in ("full", "full2d", "small_tilt"):
+        pos = probe_points(2000, 5)
+        fi, fo = os.path.join(tmp, "p.bin"), os.path.join(tmp, "z.bin")
+        pos.tofile(fi)
+        O.run_harness(["zshift", fi, fo], {"PPCTABLESDIR": ice(kind)})
+        z = np.fromfile(fo, np.float32).reshape(-1, 3)[:, :2]
+        np.savez_compressed(os.path.join(HERE, f"zshift_{kind}.npz"), pos=pos, zshift=z)
+    for case, kind, spec, photons, seed, env in RUNS:
+        info, hits, pbuf, bunch = O.harness_run(ice(kind), spec, photons, seed, os.path.join(tmp, case), env)
+        np.savez_compressed(os.path.join(HERE, f"run_{case}.npz"), hits=hits, bunch=bunch,
+                            pbuf_head=pbuf[:256], pbuf_sha=np.frombuffer(sha(pbuf.tobytes()).encode(), np.uint8),
+                            rs=np.uint64(info["rs"]), seed=np.uint32(seed), photons=np.uint32(photons),
+                            env=np.frombuffer(json.dumps(env).encode(), np.uint8))
+        print(case, info)
+
+
+if __name__ == "__main__":
+    main()

@@ -183,3 +183,28 @@ def harness_run(icedir, spec, photons, seed, prefix, env=None):
     pbuf = np.fromfile(prefix + ".pbuf", T.PBUF_DTYPE)
     bunch = np.fromfile(prefix + ".bunch", T.BUNCH_DTYPE)
     return info, hits, pbuf, bunch
+
+
+def tables_from_product(ctx):
+    """OracleTables over the product's own table image (identical values to the GPU's)."""
+    t = ctx.tables()
+    arrays = {k: t[k] for k in ("az", "lr", "ls", "is", "mcol", "sc", "lp", "absca", "wmeta", "oms")}
+    return OracleTables(ctx.params(), arrays)
+
+
+def index_probe(tb, pos):
+    """pos: (n, 8) float32 rows x,y,z,t,nx,ny,nz,length -> (ints (n,8), floats (n,2))."""
+    L = lib()
+    L.ppco_index_probe.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = len(pos)
+    oi = np.zeros((n, 8), np.int32)
+    of = np.zeros((n, 2), np.float32)
+    L.ppco_index_probe(tb.tp, ptr(pos), n, ptr(oi), ptr(of))
+    return oi, of
+
+
+def mwc_init(seed, rm):
+    """Initial stream state of every thread: (362436069 + seed, 1234567), gpu/ini.cxx:556-571."""
+    v = np.uint64((362436069 + seed) & 0xFFFFFFFF) | (np.uint64(1234567) << np.uint64(32))
+    return np.full(len(rm), v, np.uint64)

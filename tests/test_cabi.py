@@ -1,0 +1,144 @@
+"""The drop-in boundary without a GPU: the C ABI loads and exports every declared entry
+point; the C++ drop-in library exports the reference's xppc:: API (llh/ppc.h) so a program
+written against the reference header links unchanged; errors come back as the reference's
+exit statuses."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from ppc_b200 import _lib
+from ppc_b200.api import PPC, PPCError
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "ppc_b200", "lib")
+
+
+def test_c_abi_exports_every_declared_symbol():
+    L = _lib.lib()
+    hdr = open(os.path.join(ROOT, "include", "ppc_b200.h")).read()
+    declared = sorted(set(re.findall(r"\b(ppcb_[a-z_]+)\(", hdr)))
+    assert declared, "no declarations parsed"
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(declared) == set(_lib.EXPORTS)
+
+
+XPPC_API = [
+    "xppc::xrnd()", "xppc::grnd()", "xppc::start()", "xppc::stop()", "xppc::choose(int)", "xppc::ini()",
+    "xppc::fin()", "xppc::eout()", "xppc::flone(unsigned long long)", "xppc::getMaxBunchSize()",
+    "xppc::getWorkgroupSize()", "xppc::getTotalDeviceTime()", "xppc::initialize(float)",
+    "xppc::flset(int, int)", "xppc::fldir()", "xppc::flshift(float*, float*, float*)", "xppc::set_res(float)",
+    "xppc::set_res(float, float)", "xppc::efin()",
+    "xppc::sett(float, float, float, std::pair<int, unsigned long long>, int, double)",
+    "xppc::addp(float, float, float, float, float, float, int, float)",
+    "xppc::addp_clst(float, float, float, float, unsigned long long, float, float)",
+    "xppc::addp_mopo(float, float, float, float, float, float, float, float, float)",
+    "xppc::hitz", "xppc::i3oms", "xppc::omts", "xppc::hvs", "xppc::rdes", "xppc::nextgen",
+]
+
+
+def test_xppc_library_exports_reference_api():
+    out = subprocess.run(["nm", "-DC", "--defined-only", os.path.join(LIB, "libxppc.so")], capture_output=True,
+                         text=True, check=True).stdout
+    missing = [s for s in XPPC_API if s not in out]
+    assert not missing, missing
+
+
+LLH_LIKE = r"""
+#include <cmath>
+#include <map>
+#include <vector>
+#include <cstdio>
+#include HEADER
+int main(int argc, char** argv) {
+  if (argc < 2) return 0;            // linked, not run: needs a GPU
+  xppc::start();
+  xppc::initialize(1.f);
+  xppc::choose(-1);
+  xppc::ini();
+  xppc::flset(63, 20);
+  xppc::sett(0, 0, 1, std::make_pair(1, 2ULL), 0);
+  xppc::flone(1000000);
+  xppc::eout();
+  for (xppc::outz::const_iterator i = xppc::hitz.begin(); i != xppc::hitz.end(); ++i)
+    printf("%d %d %zu\n", i->first.omkey.str, i->first.omkey.dom, i->second.size());
+  xppc::efin();
+  xppc::fin();
+  xppc::stop();
+  printf("%zu %zu %g %f\n", xppc::getMaxBunchSize(), xppc::getWorkgroupSize(), xppc::getTotalDeviceTime(), xppc::xrnd());
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("header", ["ours", "reference"])
+def test_program_written_against_api_links(header, tmp_path):
+    if header == "reference":
+        h = "/root/reference/llh/ppc.h"
+        if not os.path.exists(h):
+            pytest.skip("reference header not present")
+        src = LLH_LIKE.replace("HEADER", '"' + h + '"')
+    else:
+        src = LLH_LIKE.replace("HEADER", '"' + os.path.join(ROOT, "include", "xppc.h") + '"')
+    f = tmp_path / "llh_like.cxx"
+    f.write_text(src)
+    exe = tmp_path / "llh_like"
+    r = subprocess.run(["/usr/bin/g++", "-O1", "-std=c++11", str(f), "-o", str(exe), "-L" + LIB, "-lxppc",
+                        "-Wl,-rpath," + LIB, "-Wl,--no-undefined"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_missing_configuration_reports_reference_status(tmp_path):
+    c = PPC()
+    with pytest.raises(PPCError) as e:
+        c.initialize(1.0, str(tmp_path / "nowhere"))
+    assert e.value.code == 1 and "cfg.txt" in str(e.value)
+    c.close()
+
+
+def test_corrupt_ice_table_is_rejected(tmp_path, ice_small):
+    import shutil
+    d = tmp_path / "ice"
+    shutil.copytree(ice_small, d)
+    lines = (d / "icemodel.dat").read_text().splitlines()
+    lines[5] = lines[5].split()[0] + " -1 0.01 0"  # negative scattering
+    (d / "icemodel.dat").write_text("\n".join(lines) + "\n")
+    c = PPC()
+    with pytest.raises(PPCError) as e:
+        c.initialize(1.0, str(d))
+    assert e.value.code == 1 and "Invalid value of ice parameter" in str(e.value)
+    c.close()
+
+
+def test_propagation_before_ini_is_an_error(ice_small):
+    c = PPC()
+    c.initialize(1.0, ice_small)
+    from ppc_b200 import types as T
+    b = T.bunch_led([0, 0, 0, 0], [0, 0, 1], 1, 10, 1, ka=-1, up=0, fldr=-1)
+    with pytest.raises(PPCError) as e:
+        c.propagate(b)
+    assert e.value.code == 6
+    c.close()
+
+
+def test_flasher_setup_matches_reference_semantics(ice_full, monkeypatch):
+    """flset/fldir/flshift are host-side (gpu/f2k.cxx:590-765)."""
+    monkeypatch.setenv("FLDR", "30")
+    c = PPC()
+    c.initialize(1.0, ice_full)
+    d = c.flset(40, 30)
+    assert d["r"][2] > -600 and d["r"][2] < 600
+    n = c.fldir()
+    up = np.float32(-0.2) * np.float32(np.pi / 180)
+    assert abs(n[2] - np.sin(up)) < 1e-6
+    assert abs(np.arctan2(n[1], n[0]) - np.radians(30)) < 1e-5
+    # flshift: rotating the vertical frame onto itself is the identity
+    out = c.flshift([0, 0, 1], [0.6, 0.0, 0.8])
+    assert np.allclose(out, [0.6, 0.0, 0.8])
+    out = c.flshift([1, 0, 0], [0.0, 0.0, 1.0])
+    assert np.allclose(out, [1.0, 0.0, 0.0], atol=1e-6)
+    c.close()
