@@ -6,11 +6,7 @@
 #include <string>
 
 #include "../../include/ppc_b200.h"
-#include "session.h"
-
-struct ppcb_ctx {
-  ppcb::Session s;
-};
+#include "ctx.h"
 
 static thread_local std::string g_err;
 
@@ -389,3 +385,5 @@ int ppcb_index_probe_device(ppcb_ctx* c, int device, const void* pos, int32_t n,
 }
 
 }  // extern "C"
+
+void ppcb_internal_set_error(const std::string& msg) { g_err = msg; }
