@@ -46,7 +46,7 @@ EXPORTS = [
     "ppcb_sett", "ppcb_addp", "ppcb_addp_clst", "ppcb_addp_mopo", "ppcb_flone", "ppcb_eout", "ppcb_efin",
     "ppcb_set_res", "ppcb_xrnd", "ppcb_hitz_count", "ppcb_hitz_copy", "ppcb_keep_raw", "ppcb_raw_count",
     "ppcb_raw_copy", "ppcb_last_run", "ppcb_propagate", "ppcb_propagate_device", "ppcb_rng_get", "ppcb_rng_set",
-    "ppcb_rng_reset", "ppcb_table", "ppcb_generate_device", "ppcb_index_probe_device",
+    "ppcb_rng_reset", "ppcb_table", "ppcb_generate_device", "ppcb_index_probe_device", "ppcb_propagate_noalloc",
 ]
 
 
@@ -96,6 +96,7 @@ def lib():
         "ppcb_table": (i32, [vp, C.c_char_p, P(vp), P(u64)]),
         "ppcb_generate_device": (i32, [vp, i32, vp, vp, i32, u64, vp, vp]),
         "ppcb_index_probe_device": (i32, [vp, i32, vp, i32, vp, vp, vp]),
+        "ppcb_propagate_noalloc": (i32, [vp, i32, vp, i32, u64, vp, u64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
