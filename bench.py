@@ -138,6 +138,27 @@ def cpu_reference_sample(photons_per_proc, procs, seed=0):
     return {"value": rate, "photons": photons, "seconds": secs}
 
 
+def plain_kernel_sample(photons, events, local):
+    """The reference's own CUDA kernel (gpu/pro.cu built for sm_100a with gpu/Makefile's
+    flags, oracle/_ref/ref_gpu_harness) on the same cascade workload, one eout() per event;
+    device time from the reference's own CUDA events (gpu/ppc.cu:296-304)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
+    if not os.path.exists(exe):
+        return None
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    E = photons * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
+    spec = f"cascade:12.5:-40:60:{E}:0.6:0:0.8:11"
+    env = dict(os.environ, PPCTABLESDIR=ice, CUDA_VISIBLE_DEVICES=str(local))
+    r = subprocess.run([exe, spec, str(photons), str(events), "1"], env=env, capture_output=True, text=True,
+                       timeout=600)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return None
+    x = json.loads(lines[-1])
+    x["value"] = x["photons"] / (x["device_ms"] / 1000.0)
+    return x
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -235,7 +256,7 @@ def run_ours(args, rank, world, local):
 
     # end to end through the host API: bunch upload, launch, hit download
     e2e_times, e2e_hits = [], 0
-    for k in range(args.warmup + args.steps):
+    for k in range(0 if args.no_e2e else args.warmup + args.steps):
         b, _, _ = _cascade_bunch(rng, photons, q=1, ppm=ppm)
         if dist:
             td.barrier()
@@ -246,7 +267,7 @@ def run_ours(args, rank, world, local):
         if k >= args.warmup:
             e2e_times.append(t1 - t0)
             e2e_hits += len(h)
-    e2e_total = sum(e2e_times)
+    e2e_total = sum(e2e_times) if e2e_times else float("nan")
     if dist:
         t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
         td.all_reduce(t, op=td.ReduceOp.MAX)
@@ -287,6 +308,16 @@ def run_ours(args, rank, world, local):
                      "ops_per_photon_step": ops_per_step},
         "clocks": clocks,
     }
+    if not args.no_plain_kernel:
+        del d_hits, flush
+        torch.cuda.empty_cache()
+        c.close()
+        pk = plain_kernel_sample(photons, 2, local)
+        if pk:
+            line["plain_kernel"] = {"value": pk["value"], "unit": "photons/s", "device_ms": pk["device_ms"],
+                                    "photons": pk["photons"],
+                                    "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, gpu/Makefile flags",
+                                    "speedup": value / pk["value"]}
     if not args.no_cpu_baseline:
         r = cpu_reference_sample(args.ref_photons, os.cpu_count() or 1)
         if r:
@@ -307,6 +338,8 @@ def main():
     ap.add_argument("--ref-photons", type=int, default=200_000)
     ap.add_argument("--fp32-ops-per-step", type=float, default=250.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
+    ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
