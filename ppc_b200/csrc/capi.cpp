@@ -346,7 +346,7 @@ int ppcb_table(ppcb_ctx* c, const char* name, const void** ptr, uint64_t* bytes)
 #define T(nm, vec) else if (n == nm) { p = f.vec.data(); b = f.vec.size() * sizeof(f.vec[0]); }
     if (n == "params") { p = &f.p; b = sizeof(f.p); }
     T("az", az) T("lr", lr) T("ls", ls) T("is", is) T("mcol", mcol) T("sc", sc) T("lp", lp) T("absca", absca)
-    T("wmeta", wmeta) T("oms", oms) T("rm", rm) T("wvs", wvs)
+    T("wmeta", wmeta) T("oms", oms) T("rm", rm) T("wvs", wvs) T("bfrt", bfrt)
     else if (n == "eff") { p = &f.eff; b = sizeof(f.eff); }
     else throw ppcb::Error("unknown table " + n, PPCB_EARG);
 #undef T

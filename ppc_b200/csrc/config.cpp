@@ -888,6 +888,22 @@ void Config::load(const std::string& tables_dir) {
     for (int i = 0; i < k; i++) env.sum[i] /= sum;
   }
 
+  // Birefringence angular functions of gpu/pro.cu:784-786 (without the sqrt(ra), rb
+  // factors), tabulated in double precision against v = sqrt(1 - |cos|) of the angle to
+  // the anisotropy axis: with cos = 1 - v^2 and sin = v*sqrt(2 - v^2) all three are smooth
+  // in v, so linear interpolation on 512 intervals is accurate to ~1e-7 relative.
+  bfrt.assign((PPCB_BFR_TAB + 1) * 4, 0.f);
+  for (int k = 0; k <= PPCB_BFR_TAB; k++) {
+    const double v = (double)k / PPCB_BFR_TAB, c = 1 - v * v, s = v * std::sqrt(2 - v * v);
+    const float* b = p.bfr;
+    double sx = std::max(0.0, b[0] * std::exp(-b[1] * std::pow(std::atan(b[3] * s), (double)b[2])));
+    double sy = std::max(0.0, b[4] * std::exp(-b[5] * std::pow(std::atan(b[7] * s), (double)b[6])));
+    double mx = std::max(0.0, b[8] * std::atan(b[11] * s * c) * std::exp(-b[9] * s + b[10] * c));
+    bfrt[k * 4 + 0] = (float)sx;
+    bfrt[k * 4 + 1] = (float)sy;
+    bfrt[k * 4 + 2] = (float)mx;
+  }
+
   // ice optical properties, gpu/ini.cxx:1494-1696
   const float wv0 = 400;
   float A, B, D, E, a, k;

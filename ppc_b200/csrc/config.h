@@ -120,6 +120,7 @@ class Config {
   std::vector<ppcb_wmeta> wmeta;           // [WNUM]
   std::vector<ppcb_dom> oms;               // [gsize]
   std::vector<uint32_t> rm;                // [rsize]
+  std::vector<float> bfrt;                 // [(BFR_TAB+1)*4] birefringence functions of v = sqrt(1-|cos|)
 
   // ---- host-side tables ----
   std::vector<OMName> names;               // [gsize]

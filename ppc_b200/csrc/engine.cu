@@ -133,6 +133,8 @@ void Engine::ini() {
     upload(g.is, cfg.is.data(), PPCB_CX * PPCB_CY, "is");
     g.mcol = dalloc<int8_t>(PPCB_CTX * PPCB_CTY, "mcol");
     upload(g.mcol, cfg.mcol.data(), PPCB_CTX * PPCB_CTY, "mcol");
+    g.bfrt = dalloc<float4>(PPCB_BFR_TAB + 1, "bfrt");
+    upload(g.bfrt, (const float4*)cfg.bfrt.data(), PPCB_BFR_TAB + 1, "bfrt");
     g.rs = dalloc<uint64_t>(g.T, "rs");
     g.rm = dalloc<uint32_t>(g.T, "rm");
     upload(g.rm, cfg.rm.data(), g.T, "rm");
@@ -174,9 +176,10 @@ void Engine::free_device(DeviceCtx& g) {
   cudaSetDevice(g.dev);
   if (g.st) cudaStreamSynchronize(g.st);
   if (g.cp) cudaStreamSynchronize(g.cp);
-  void* ptrs[] = {g.absca, g.wmeta, g.lp, g.oms, g.az, g.sc, g.lr, g.ls, g.is, g.mcol, g.rs, g.rm};
+  void* ptrs[] = {g.absca, g.wmeta, g.lp, g.oms, g.az, g.sc, g.lr, g.ls, g.is, g.mcol, g.bfrt, g.rs, g.rm};
   for (void* p : ptrs) if (p) cudaFree(p);
   g.absca = nullptr; g.wmeta = nullptr; g.lp = nullptr; g.oms = nullptr; g.az = nullptr; g.sc = nullptr;
+  g.bfrt = nullptr;
   g.lr = nullptr; g.ls = nullptr; g.is = nullptr; g.mcol = nullptr; g.rs = nullptr; g.rm = nullptr;
   for (auto& S : g.slot) {
     if (S.bunches) cudaFree(S.bunches);
@@ -211,7 +214,7 @@ KArgs Engine::args_for(int d) const {
   memset(&a, 0, sizeof(a));
   a.p = cfg.p;
   a.absca = g.absca; a.wmeta = g.wmeta; a.lp = g.lp; a.oms = g.oms; a.az = g.az; a.sc = g.sc;
-  a.lr = g.lr; a.ls = g.ls; a.is = g.is; a.mcol = g.mcol;
+  a.lr = g.lr; a.ls = g.ls; a.is = g.is; a.mcol = g.mcol; a.bfrt = g.bfrt;
   a.rs = g.rs; a.rm = g.rm;
   a.deterministic = deterministic ? 1 : 0;
   a.max_steps = max_steps;

@@ -43,6 +43,7 @@ struct DeviceCtx {
   uint16_t* ls = nullptr;
   uint16_t* is = nullptr;
   int8_t* mcol = nullptr;
+  float4* bfrt = nullptr;
   uint64_t* rs = nullptr;
   uint32_t* rm = nullptr;
   struct Slot {

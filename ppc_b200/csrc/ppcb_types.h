@@ -25,6 +25,8 @@
 #define PPCB_MAXGEO 16384   // optical modules
 #define PPCB_MAXRND 131072  // MWC multipliers (one random stream per GPU thread)
 
+#define PPCB_BFR_TAB 1024   // intervals of the tabulated birefringence angular functions
+
 #define PPCB_XXX 1.e-5f
 #define PPCB_FPI 3.141592653589793f
 #define PPCB_OMR 0.16510f   // DOM radius [m]

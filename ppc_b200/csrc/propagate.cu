@@ -42,6 +42,7 @@ struct SmemTables {
   uint16_t ls[PPCB_NSTR];
   uint16_t is[PPCB_CX * PPCB_CY];
   int8_t mcol[PPCB_CTX * PPCB_CTY];
+  float4 bfrt[PPCB_BFR_TAB + 1];  // birefringence angular functions (sx, sy, mx, -)
 };
 
 // ---------------------------------------------------------------- IEEE helpers
@@ -588,12 +589,19 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
       if (ra < 0) ra = 0;
       if (rb < 0) rb = 0;
       float dot = e.azx * n.x + e.azy * n.y;
-      float sdt = sqrtf(1 - dot * dot);
-      float cdt = fabsf(dot);
-      const float* bf = e.bfr;
-      float sx = sqrtf(ra) * fmaxf(0.f, bf[0] * expf(-bf[1] * powf(atanf(bf[3] * sdt), bf[2])));
-      float sy = sqrtf(ra) * fmaxf(0.f, bf[4] * expf(-bf[5] * powf(atanf(bf[7] * sdt), bf[6])));
-      float mx = rb * fmaxf(0.f, bf[8] * atanf(bf[11] * sdt * cdt) * expf(-bf[9] * sdt + bf[10] * cdt));
+      // angular diffusion functions of gpu/pro.cu:784-786, tabulated on the host in
+      // v = sqrt(1 - |dot|) (smooth in v at both ends) and interpolated linearly
+      float sx, sy, mx;
+      {
+        const float v = sqrtf(fmaxf(0.f, 1.f - fabsf(dot))) * PPCB_BFR_TAB;
+        const int iv = min((int)v, PPCB_BFR_TAB - 1);
+        const float fv = v - iv;
+        const float4 t0 = S.bfrt[iv], t1 = S.bfrt[iv + 1];
+        const float sra = sqrtf(ra);
+        sx = sra * fmaf(fv, t1.x - t0.x, t0.x);
+        sy = sra * fmaf(fv, t1.y - t0.y, t0.y);
+        mx = rb * fmaf(fv, t1.z - t0.z, t0.z);
+      }
       float qx = e.azx - dot * n.x, qy = e.azy - dot * n.y, qz = -dot * n.z;
       if (dot < 0) { qx = -qx; qy = -qy; qz = -qz; }
       float qn = qx * qx + qy * qy + qz * qz;
@@ -685,18 +693,34 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
   for (int i = t; i < PPCB_NSTR; i += nt) S.ls[i] = a.ls[i];
   for (int i = t; i < PPCB_CX * PPCB_CY; i += nt) S.is[i] = a.is[i];
   for (int i = t; i < PPCB_CTX * PPCB_CTY; i += nt) S.mcol[i] = a.mcol[i];
+  for (int i = t; i <= PPCB_BFR_TAB; i += nt) S.bfrt[i] = a.bfrt[i];
   __syncthreads();
 }
 
 #define PPCB_BLOCK 256
 #define PPCB_MINB 3
 
+// Per-warp pool of sampled photons (photon regrouping by state).  Sampling a photon is
+// long and branchy (source type, gamma profile, Cherenkov cone); done by the one or two
+// lanes whose photon just died it runs at 1/32 SIMT efficiency.  Instead the whole warp
+// samples up to 32 photons at once into the pool, and lanes whose photon died take one
+// from the pool (three 16-byte shared-memory loads).
+struct PhotonPool {
+  float4 r[32];
+  float4 n[32];
+  int4 m[32];  // wavelength bin, segment, flasher DOM, veto code
+  int count;
+};
+
 __global__ void __launch_bounds__(PPCB_BLOCK, PPCB_MINB) k_propagate(const __grid_constant__ KArgs a) {
   __shared__ SmemTables S;
+  __shared__ PhotonPool pools[PPCB_BLOCK / 32];
   load_tables(a, S);
   const uint32_t T = gridDim.x * blockDim.x;
   const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned int lane = threadIdx.x & 31;
+  const unsigned int FULL = 0xffffffffu;
+  PhotonPool& P = pools[threadIdx.x >> 5];
   Rng s;
   {
     uint64_t st = a.rs[gt];
@@ -704,42 +728,84 @@ __global__ void __launch_bounds__(PPCB_BLOCK, PPCB_MINB) k_propagate(const __gri
   }
   Photon ph;
   bool alive = false;
+  bool exhausted = false;   // warp-uniform: no photons left to sample
+  int have = 0;             // warp-uniform: photons in the pool
   uint64_t sidx = gt;
   int hint = 0;
   unsigned long long nsteps = 0;
   unsigned int nan_steps = 0, capped = 0;
+  // every lane of the warp stays in this loop until the warp is done, so the warp-wide
+  // operations below always see all 32 lanes
   while (true) {
-    uint64_t idx = ~0ull;
-    if (a.deterministic) {
-      if (!alive) { idx = sidx; sidx += T; }
-    } else {
-      const unsigned int am = __activemask();
-      const unsigned int need = __ballot_sync(am, !alive);
-      if (need) {
-        const int leader = __ffs(need) - 1;
-        unsigned long long base = 0;
-        if ((int)lane == leader) base = atomicAdd(&a.ctrl->next, (unsigned long long)__popc(need));
-        base = __shfl_sync(am, base, leader);
-        if (!alive) idx = base + __popc(need & ((1u << lane) - 1u));
+    const unsigned int dead = __ballot_sync(FULL, !alive);
+    if (dead && !(exhausted && have == 0)) {
+      // --- sample: each generating lane produces one photon from its own stream
+      bool gen = false;
+      uint64_t gidx = 0;
+      unsigned long long base = 0;
+      int ngen = 0;
+      if (a.deterministic) {  // photon i on thread i mod T, as the oracle sequences it
+        gen = !alive && sidx < a.num;
+        gidx = sidx;
+        if (!alive) sidx += T;
+      } else if (have < __popc(dead) && !exhausted) {
+        ngen = 32 - have;
+        if (lane == 0) base = atomicAdd(&a.ctrl->next, (unsigned long long)ngen);
+        base = __shfl_sync(FULL, base, 0);
+        gidx = base + lane;
+        gen = (int)lane < ngen && gidx < a.num;
+        if (base + ngen >= a.num) exhausted = true;
+      }
+      Photon g;
+      if (gen) {
+        hint = find_bunch(a, gidx, hint);
+        const ppcb_bunch p = a.bunches[hint];
+        generate(a, p, s, g);
+      }
+      if (a.deterministic) {
+        if (gen) { ph = g; alive = true; }
+        exhausted = __all_sync(FULL, sidx >= a.num);
+      } else {
+        if (gen) {
+          const int slot = have + lane;
+          P.r[slot] = g.r;
+          P.n[slot] = g.n;
+          P.m[slot] = make_int4(g.wl, (int)g.niw, g.om0, g.ofla);
+        }
+        have += __popc(__ballot_sync(FULL, gen));
+        __syncwarp();
+        // --- hand out: the k-th dead lane takes the k-th photon from the top of the pool
+        const int rank = __popc(dead & ((1u << lane) - 1u));
+        if (!alive && rank < have) {
+          const int slot = have - 1 - rank;
+          ph.r = P.r[slot];
+          ph.n = P.n[slot];
+          const int4 m = P.m[slot];
+          ph.wl = m.x; ph.niw = (uint32_t)m.y; ph.om0 = m.z; ph.ofla = m.w;
+          alive = true;
+        }
+        have -= min(have, __popc(dead));
+        __syncwarp();
+      }
+      if (alive && (dead >> lane & 1u)) {  // a fresh photon: absorption depth, gpu/pro.cu:496-497
+        ph.TOT = -logf(xrnd(s));
+        ph.SCA = 0;
+        ph.old = -1;
+        ph.steps = 0;
+        if (ph.ofla < -1) ph.TOT = 0;
       }
     }
-    if (!alive) {
-      if (idx >= a.num) break;
-      hint = find_bunch(a, idx, hint);
-      const ppcb_bunch p = a.bunches[hint];
-      generate(a, p, s, ph);
-      ph.TOT = -logf(xrnd(s));
-      ph.SCA = 0;
-      ph.old = -1;
-      ph.steps = 0;
-      if (ph.ofla < -1) ph.TOT = 0;
-      alive = true;
+    if (!__any_sync(FULL, alive)) {
+      if (exhausted && have == 0) break;
+      continue;
     }
-    step(a, S, ph, s, nan_steps);
-    ph.steps++;
-    nsteps++;
-    if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) { ph.TOT = 0; capped++; }
-    if (ph.TOT == 0) alive = false;
+    if (alive) {
+      step(a, S, ph, s, nan_steps);
+      ph.steps++;
+      nsteps++;
+      if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) { ph.TOT = 0; capped++; }
+      if (ph.TOT == 0) alive = false;
+    }
   }
   a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
   atomicAdd(&a.ctrl->steps, nsteps);

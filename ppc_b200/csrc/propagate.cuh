@@ -21,6 +21,7 @@ struct KArgs {
   const uint16_t* ls;        // [NSTR]        -> shared memory
   const uint16_t* is;        // [CX*CY]       -> shared memory
   const int8_t* mcol;        // [CTX*CTY]     -> shared memory
+  const float4* bfrt;        // [BFR_TAB+1]   -> shared memory
   // work
   const ppcb_bunch* bunches; // [nb]
   const uint64_t* bstart;    // [nb+1] first photon index of each bunch (exclusive prefix sum)

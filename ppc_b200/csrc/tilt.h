@@ -41,9 +41,16 @@ template <class Tab>
 PPCB_HD float zshift_t(const ppcb_params& d, const Tab& t, float rx, float ry, float rz, float& dz) {
   if (d.tmod == 1) {  // 1-d: interpolate between the two maps bracketing the distance along 225 deg
     float nr = PPCB_SUB(PPCB_ADD(PPCB_MUL(d.lnx, rx), PPCB_MUL(d.lny, ry)), d.r0);
+    // first j >= 1 with nr < lr[j], or j = lnum-1.  The radii are non-decreasing (checked
+    // when loaded), so that is 1 + #{k in [1, lnum-2] : !(nr < lr[k])}: a loop with the same
+    // trip count for every thread (NaN counts as "not below", as in the search loop).
     int j = 1;
-    for (; j < PPCB_LMAX; j++) if (nr < t.lr(j) || j == d.lnum - 1) break;
-    if (j >= PPCB_LMAX) j = PPCB_LMAX - 1;  // a single-map table would run off the end
+    if (d.lnum >= 2) {
+      for (int k = 1; k < d.lnum - 1; k++) j += !(nr < t.lr(k));
+    } else {
+      for (; j < PPCB_LMAX; j++) if (nr < t.lr(j)) break;
+      if (j >= PPCB_LMAX) j = PPCB_LMAX - 1;  // a single-map table would run off the end
+    }
     float z = PPCB_MUL(PPCB_SUB(rz, d.lmin), d.lrdz);
     int i = j - 1, k = tmin(tmax(PPCB_FLOOR_I(z), 0), d.lpts);
     const float2 pi = t.lp(i, k), pj = t.lp(j, k);
