@@ -146,6 +146,41 @@ int ppcb_generate_device(ppcb_ctx* c, int device, const ppcb_bunch* bunches, con
 int ppcb_index_probe_device(ppcb_ctx* c, int device, const void* pos, int32_t n, int32_t* out_i, float* out_f,
                             void* stream);
 
+/* ---- batched events ----
+ * No counterpart in the reference, which propagates one source per eout()
+ * (gpu/f2k.cxx:536-541).  Thousands of events with uneven photon counts run in one
+ * persistent, work-stealing launch, replayed from a CUDA graph; each event's hits go to
+ * its own region of the hit buffer, sized as photons x hits_per_photon + 64 slots (an
+ * upper bound: hits beyond it are counted in `overflowed`, not stored).  Bunch .q is the
+ * event index in [0, events).  The buffers are sized once at creation. */
+typedef struct ppcb_batch ppcb_batch;
+typedef struct ppcb_batch_info {
+  uint64_t photons, steps;
+  uint64_t hits;        /* produced */
+  uint64_t kept;        /* stored */
+  uint32_t overflowed;  /* events whose region was too small */
+  uint32_t pad_;
+  double device_ms;     /* the propagation kernel */
+  double graph_ms;      /* uploads, kernel, compaction and downloads */
+} ppcb_batch_info;
+typedef struct ppcb_tune_info {
+  int32_t threads, blocks_per_sm, refill_below, pad_;
+  double photons_per_s;
+} ppcb_tune_info;
+int ppcb_batch_create(ppcb_ctx* c, int device, uint32_t max_events, uint32_t max_bunches, uint64_t hit_capacity,
+                      ppcb_batch** out);
+int ppcb_batch_destroy(ppcb_batch* b);
+int ppcb_batch_set_graph(ppcb_batch* b, int use_graph);
+int ppcb_batch_run(ppcb_batch* b, const ppcb_bunch* bunches, int32_t nb, uint32_t events, double hits_per_photon,
+                   ppcb_batch_info* info);
+/* per event of the last run: hits produced, and offsets (events+1) into the kept hits */
+int ppcb_batch_counts(ppcb_batch* b, uint32_t* produced, uint64_t* offsets);
+int ppcb_batch_hits(ppcb_batch* b, ppcb_hit* out, uint64_t cap, uint64_t* n);
+/* Times the kernel's launch shapes (threads per block, blocks per SM, photon-pool refill
+ * threshold) on a scaled-down copy of the batch and keeps the fastest for this context. */
+int ppcb_batch_autotune(ppcb_batch* b, const ppcb_bunch* bunches, int32_t nb, uint32_t events, uint64_t sample_photons,
+                        ppcb_tune_info* out);
+
 /* ---- propagation that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device memory while
  * they run: frameworks that reserve the GPU's memory for their own pool at start-up, and

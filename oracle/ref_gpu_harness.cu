@@ -44,7 +44,40 @@ int main(int argc, char** argv) {
   }
   auto t0 = std::chrono::steady_clock::now();
   unsigned long long done = 0, nhits = 0;
-  for (int ev = 0; ev < events; ev++) {
+  if (tok[0] == "file") {
+    // one event per line: "F <str> <om> <photons>" (flasher set up by flset from FLDR/ELEV)
+    // or "C <x> <y> <z> <E> <nx> <ny> <nz> <photons>" (EM cascade)
+    FILE* f = fopen(tok[1].c_str(), "r");
+    if (!f) { perror(tok[1].c_str()); return 2; }
+    char kind[4];
+    int ev = 0;
+    while (fscanf(f, "%3s", kind) == 1) {
+      unsigned long long n = 0;
+      if (kind[0] == 'F') {
+        int str, om;
+        if (fscanf(f, "%d %d %llu", &str, &om, &n) != 3) break;
+        flset(str, om);
+      } else {
+        float x, y, zz, E, nx, ny, nz;
+        if (fscanf(f, "%f %f %f %f %f %f %f %llu", &x, &y, &zz, &E, &nx, &ny, &nz, &n) != 8) break;
+        p.r.x = x; p.r.y = y; p.r.z = zz; p.r.w = 0;
+        p.n.x = nx; p.n.y = ny; p.n.z = nz;
+        p.type = -11; p.beta = 1; p.tau = 0;
+        yield(E, 0, 11);
+      }
+      mcid id; id.first = ev; id.second = 0; id.frame = 0; id.t0 = 0;
+      flnz.push_back(id); finc(); p.q = flne;
+      addh(n);
+      eout();
+      for (auto i = hitz.begin(); i != hitz.end(); ++i) nhits += i->second.size();
+      efin();
+      done += n;
+      ev++;
+    }
+    fclose(f);
+    events = ev;
+  }
+  for (int ev = 0; ev < events && tok[0] != "file"; ev++) {
     if (tok[0] == "cascade") {
       p.r.x = atof(tok[1].c_str()); p.r.y = atof(tok[2].c_str()); p.r.z = atof(tok[3].c_str()); p.r.w = 0;
       p.n.x = atof(tok[5].c_str()); p.n.y = atof(tok[6].c_str()); p.n.z = atof(tok[7].c_str());

@@ -30,6 +30,16 @@ class Info(C.Structure):
                 ("ovr", C.c_uint32), ("seed", C.c_uint32), ("nextgen", C.c_int32)]
 
 
+class BatchInfo(C.Structure):
+    _fields_ = [("photons", C.c_uint64), ("steps", C.c_uint64), ("hits", C.c_uint64), ("kept", C.c_uint64),
+                ("overflowed", C.c_uint32), ("pad_", C.c_uint32), ("device_ms", C.c_double), ("graph_ms", C.c_double)]
+
+
+class TuneInfo(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("refill_below", C.c_int32),
+                ("pad_", C.c_int32), ("photons_per_s", C.c_double)]
+
+
 class Dom(C.Structure):
     _fields_ = [("R", C.c_float), ("F", C.c_float), ("r", C.c_float * 3)]
 
@@ -47,6 +57,8 @@ EXPORTS = [
     "ppcb_set_res", "ppcb_xrnd", "ppcb_hitz_count", "ppcb_hitz_copy", "ppcb_keep_raw", "ppcb_raw_count",
     "ppcb_raw_copy", "ppcb_last_run", "ppcb_propagate", "ppcb_propagate_device", "ppcb_rng_get", "ppcb_rng_set",
     "ppcb_rng_reset", "ppcb_table", "ppcb_generate_device", "ppcb_index_probe_device", "ppcb_propagate_noalloc",
+    "ppcb_batch_create", "ppcb_batch_destroy", "ppcb_batch_set_graph", "ppcb_batch_run", "ppcb_batch_counts",
+    "ppcb_batch_hits", "ppcb_batch_autotune",
 ]
 
 
@@ -97,6 +109,13 @@ def lib():
         "ppcb_generate_device": (i32, [vp, i32, vp, vp, i32, u64, vp, vp]),
         "ppcb_index_probe_device": (i32, [vp, i32, vp, i32, vp, vp, vp]),
         "ppcb_propagate_noalloc": (i32, [vp, i32, vp, i32, u64, vp, u64, vp, vp]),
+        "ppcb_batch_create": (i32, [vp, i32, u32, u32, u64, P(vp)]),
+        "ppcb_batch_destroy": (i32, [vp]),
+        "ppcb_batch_set_graph": (i32, [vp, i32]),
+        "ppcb_batch_run": (i32, [vp, vp, i32, u32, f64, P(BatchInfo)]),
+        "ppcb_batch_counts": (i32, [vp, vp, vp]),
+        "ppcb_batch_hits": (i32, [vp, vp, u64, P(u64)]),
+        "ppcb_batch_autotune": (i32, [vp, vp, i32, u32, u64, P(TuneInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -204,3 +204,59 @@ class PPC:
             "absca": b("absca", "<f4"), "wmeta": b("wmeta", "<f4"), "oms": b("oms", T.DOM_DTYPE),
             "rm": b("rm", "<u4"), "wvs": b("wvs", "<f4"), "eff": b("eff", "<f4"),
         }
+
+
+class Batch:
+    """Many events in one launch (ppcb_batch_*): bunch .q = event index in [0, events)."""
+
+    def __init__(self, ctx, max_events, max_bunches, hit_capacity, device=0):
+        from ._lib import BatchInfo, TuneInfo  # noqa: F401
+        self._ctx = ctx
+        self._b = C.c_void_p()
+        check(lib().ppcb_batch_create(ctx._c, device, int(max_events), int(max_bunches), int(hit_capacity),
+                                      C.byref(self._b)))
+        self.events = 0
+
+    def set_graph(self, use):
+        check(lib().ppcb_batch_set_graph(self._b, int(bool(use))))
+
+    def run(self, bunches, events, hits_per_photon=0.02):
+        from ._lib import BatchInfo
+        bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
+        info = BatchInfo()
+        check(lib().ppcb_batch_run(self._b, _p(bunches), len(bunches), int(events), float(hits_per_photon),
+                                   C.byref(info)))
+        self.events = int(events)
+        return {k: getattr(info, k) for k, _ in BatchInfo._fields_ if k != "pad_"}
+
+    def counts(self):
+        produced = np.zeros(self.events, np.uint32)
+        offsets = np.zeros(self.events + 1, np.uint64)
+        check(lib().ppcb_batch_counts(self._b, _p(produced), _p(offsets)))
+        return produced, offsets
+
+    def hits(self):
+        n = C.c_uint64()
+        check(lib().ppcb_batch_hits(self._b, None, 0, C.byref(n)))
+        out = np.zeros(n.value, T.HIT_DTYPE)
+        check(lib().ppcb_batch_hits(self._b, _p(out), n.value, C.byref(n)))
+        return out
+
+    def autotune(self, bunches, events, sample_photons=20_000_000):
+        from ._lib import TuneInfo
+        bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
+        t = TuneInfo()
+        check(lib().ppcb_batch_autotune(self._b, _p(bunches), len(bunches), int(events), int(sample_photons),
+                                        C.byref(t)))
+        return {k: getattr(t, k) for k, _ in TuneInfo._fields_ if k != "pad_"}
+
+    def close(self):
+        if self._b:
+            lib().ppcb_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

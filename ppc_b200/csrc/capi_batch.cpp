@@ -1,0 +1,110 @@
+// C ABI of the batched launch (declarations: include/ppc_b200.h, "batched events").
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "../../include/ppc_b200.h"
+#include "batch.h"
+#include "ctx.h"
+
+struct ppcb_batch {
+  ppcb::Batch* b = nullptr;
+  ppcb::BatchResult last;
+  uint32_t events = 0;
+};
+
+template <class F>
+static int bguard(F&& f) {
+  try {
+    f();
+    return PPCB_OK;
+  } catch (const ppcb::Error& e) {
+    ppcb_internal_set_error(e.what());
+    return e.code ? e.code : PPCB_ECONFIG;
+  } catch (const std::exception& e) {
+    ppcb_internal_set_error(e.what());
+    return PPCB_EARG;
+  }
+}
+
+extern "C" {
+
+int ppcb_batch_create(ppcb_ctx* c, int device, uint32_t max_events, uint32_t max_bunches, uint64_t hit_capacity,
+                      ppcb_batch** out) {
+  if (!c || !out) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    ppcb_batch* x = new ppcb_batch();
+    try {
+      x->b = new ppcb::Batch(c->s.eng, device, max_events, max_bunches, hit_capacity);
+    } catch (...) {
+      delete x;
+      throw;
+    }
+    *out = x;
+  });
+}
+
+int ppcb_batch_destroy(ppcb_batch* x) {
+  if (!x) return PPCB_OK;
+  int r = bguard([&] { delete x->b; });
+  delete x;
+  return r;
+}
+
+int ppcb_batch_set_graph(ppcb_batch* x, int use_graph) {
+  if (!x) { ppcb_internal_set_error("null batch"); return PPCB_EARG; }
+  x->b->use_graph = use_graph != 0;
+  return PPCB_OK;
+}
+
+int ppcb_batch_run(ppcb_batch* x, const ppcb_bunch* bunches, int32_t nb, uint32_t events, double hits_per_photon,
+                   ppcb_batch_info* info) {
+  if (!x || !bunches) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    x->b->run(bunches, nb, events, x->last, hits_per_photon);
+    x->events = events;
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->photons = x->last.photons;
+      info->steps = x->last.steps;
+      info->kept = x->last.hits.size();
+      uint64_t produced = 0;
+      for (uint32_t v : x->last.produced) produced += v;
+      info->hits = produced;
+      info->overflowed = x->last.overflowed;
+      info->device_ms = x->last.device_ms;
+      info->graph_ms = x->last.graph_ms;
+    }
+  });
+}
+
+int ppcb_batch_counts(ppcb_batch* x, uint32_t* produced, uint64_t* offsets) {
+  if (!x) { ppcb_internal_set_error("null batch"); return PPCB_EARG; }
+  if (produced) memcpy(produced, x->last.produced.data(), x->events * sizeof(uint32_t));
+  if (offsets) memcpy(offsets, x->last.offset.data(), (x->events + 1) * sizeof(uint64_t));
+  return PPCB_OK;
+}
+
+int ppcb_batch_hits(ppcb_batch* x, ppcb_hit* out, uint64_t cap, uint64_t* n) {
+  if (!x) { ppcb_internal_set_error("null batch"); return PPCB_EARG; }
+  uint64_t k = std::min<uint64_t>(cap, x->last.hits.size());
+  if (k && out) memcpy(out, x->last.hits.data(), k * sizeof(ppcb_hit));
+  if (n) *n = x->last.hits.size();
+  return PPCB_OK;
+}
+
+int ppcb_batch_autotune(ppcb_batch* x, const ppcb_bunch* bunches, int32_t nb, uint32_t events, uint64_t sample_photons,
+                        ppcb_tune_info* out) {
+  if (!x || !bunches) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    ppcb::TuneResult t = x->b->autotune(bunches, nb, events, sample_photons);
+    if (out) {
+      out->threads = t.threads;
+      out->blocks_per_sm = t.blocks_per_sm;
+      out->refill_below = t.refill_below;
+      out->photons_per_s = t.photons_per_s;
+    }
+  });
+}
+
+}  // extern "C"

@@ -10,7 +10,6 @@
 
 namespace ppcb {
 
-static const int kBlock = 256;
 static const int kOver = 128;   // minimum photons per bunch slot (gpu/ini.cxx:18)
 static const int kNpho = 1024;  // photons per thread per launch (gpu/ini.cxx:21)
 
@@ -81,6 +80,7 @@ void Engine::ini() {
     DeviceCtx& g = devs[k];
     int npho = g.T;
     check(cudaSetDevice(g.dev), "cudaSetDevice");
+    const int kBlock = threads_per_block == 128 ? 128 : 256;
     int per_sm = blocks_per_sm > 0 ? blocks_per_sm : propagate_max_blocks_per_sm(kBlock);
     if (const char* b = getenv("PPCB_BLOCKS_PER_SM")) if (atoi(b) > 0) per_sm = atoi(b);
     if (per_sm <= 0) per_sm = 1;
@@ -218,6 +218,7 @@ KArgs Engine::args_for(int d) const {
   a.rs = g.rs; a.rm = g.rm;
   a.deterministic = deterministic ? 1 : 0;
   a.max_steps = max_steps;
+  a.refill_below = refill_below;
   return a;
 }
 

@@ -78,6 +78,8 @@ class Engine {
   uint64_t pmax = 0, pmxo = 0;     // photons / bunches per launch
   unsigned int hquo = 1;
   int blocks_per_sm = 0;           // 0: occupancy maximum
+  int threads_per_block = 256;     // 256 or 128 (compiled shapes of the kernel)
+  int refill_below = 0;            // photon pool refill threshold (0: refill on demand)
 
   void initialize(const std::string& dir, float enh);
   void choose(int device);         // -1: every visible device

@@ -216,10 +216,10 @@ struct Photon {
   uint32_t steps;
 };
 
-__device__ __forceinline__ int find_bunch(const KArgs& a, uint64_t i, int hint) {
+__device__ __forceinline__ int find_bunch(const KArgs& a, int nb, uint64_t i, int hint) {
   // exclusive prefix sums: bunch k holds photons [bstart[k], bstart[k+1])
-  if (hint >= 0 && hint < a.nb && __ldg(&a.bstart[hint]) <= i && i < __ldg(&a.bstart[hint + 1])) return hint;
-  int lo = 0, hi = a.nb - 1;
+  if (hint >= 0 && hint < nb && __ldg(&a.bstart[hint]) <= i && i < __ldg(&a.bstart[hint + 1])) return hint;
+  int lo = 0, hi = nb - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
     if (__ldg(&a.bstart[mid]) <= i) lo = mid;
@@ -355,6 +355,17 @@ __device__ __forceinline__ void generate(const KArgs& a, const ppcb_bunch& p, Rn
 __device__ __forceinline__ float2 ice(const float2* __restrict__ t, int J) { return __ldg(&t[J]); }
 
 __device__ __forceinline__ void emit_hit(const KArgs& a, const ppcb_hit& h) {
+  if (a.ev_cnt) {  // batched launch: the event's own region, sized from an upper bound
+    const unsigned int e = h.n;
+    const unsigned int slot = atomicAdd(&a.ev_cnt[e], 1u);
+    if (slot < __ldg(&a.ev_cap[e])) {
+      uint4* dst = reinterpret_cast<uint4*>(&a.hits[__ldg(&a.ev_off[e]) + slot]);
+      const uint4* src = reinterpret_cast<const uint4*>(&h);
+      dst[0] = src[0];
+      dst[1] = src[1];
+    }
+    return;
+  }
   cg::coalesced_group g = cg::coalesced_threads();
   unsigned long long base = 0;
   if (g.thread_rank() == 0) base = atomicAdd(&a.ctrl->hidx, (unsigned long long)g.size());
@@ -698,7 +709,6 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
 }
 
 #define PPCB_BLOCK 256
-#define PPCB_MINB 3
 
 // Per-warp pool of sampled photons (photon regrouping by state).  Sampling a photon is
 // long and branchy (source type, gamma profile, Cherenkov cone); done by the one or two
@@ -712,10 +722,14 @@ struct PhotonPool {
   int count;
 };
 
-__global__ void __launch_bounds__(PPCB_BLOCK, PPCB_MINB) k_propagate(const __grid_constant__ KArgs a) {
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant__ KArgs a) {
   __shared__ SmemTables S;
-  __shared__ PhotonPool pools[PPCB_BLOCK / 32];
+  __shared__ PhotonPool pools[BLOCK / 32];
   load_tables(a, S);
+  // launch sizes: from the parameters, or from device memory for replayed graphs
+  const uint64_t num = a.dyn ? a.dyn[0] : a.num;
+  const int nb = a.dyn ? (int)a.dyn[1] : a.nb;
   const uint32_t T = gridDim.x * blockDim.x;
   const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned int lane = threadIdx.x & 31;
@@ -745,26 +759,26 @@ __global__ void __launch_bounds__(PPCB_BLOCK, PPCB_MINB) k_propagate(const __gri
       unsigned long long base = 0;
       int ngen = 0;
       if (a.deterministic) {  // photon i on thread i mod T, as the oracle sequences it
-        gen = !alive && sidx < a.num;
+        gen = !alive && sidx < num;
         gidx = sidx;
         if (!alive) sidx += T;
-      } else if (have < __popc(dead) && !exhausted) {
+      } else if ((have < __popc(dead) || have < a.refill_below) && !exhausted) {
         ngen = 32 - have;
         if (lane == 0) base = atomicAdd(&a.ctrl->next, (unsigned long long)ngen);
         base = __shfl_sync(FULL, base, 0);
         gidx = base + lane;
-        gen = (int)lane < ngen && gidx < a.num;
-        if (base + ngen >= a.num) exhausted = true;
+        gen = (int)lane < ngen && gidx < num;
+        if (base + ngen >= num) exhausted = true;
       }
       Photon g;
       if (gen) {
-        hint = find_bunch(a, gidx, hint);
+        hint = find_bunch(a, nb, gidx, hint);
         const ppcb_bunch p = a.bunches[hint];
         generate(a, p, s, g);
       }
       if (a.deterministic) {
         if (gen) { ph = g; alive = true; }
-        exhausted = __all_sync(FULL, sidx >= a.num);
+        exhausted = __all_sync(FULL, sidx >= num);
       } else {
         if (gen) {
           const int slot = have + lane;
@@ -819,7 +833,7 @@ __global__ void __launch_bounds__(PPCB_BLOCK) k_generate(const __grid_constant__
   Rng s;
   uint64_t st = a.rs[gt];
   s.x = (uint32_t)st; s.y = (uint32_t)(st >> 32); s.a = a.rm[gt];
-  int b = find_bunch(a, gt, 0);
+  int b = find_bunch(a, a.nb, gt, 0);
   const ppcb_bunch p = a.bunches[b];
   Photon ph;
   generate(a, p, s, ph);
@@ -858,9 +872,12 @@ __global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos
   of[2 * k + 1] = dz;
 }
 
+// Two compiled shapes: 256 threads x 3 blocks per SM and 128 x 6 (the same 768 threads
+// per SM at <= 80 registers); the autotuner picks one.
 cudaError_t launch_propagate(const KArgs& a, LaunchShape sh, cudaStream_t st) {
-  if (sh.threads != PPCB_BLOCK) return cudaErrorInvalidConfiguration;
-  k_propagate<<<sh.blocks, sh.threads, 0, st>>>(a);
+  if (sh.threads == 256) k_propagate<256, 3><<<sh.blocks, 256, 0, st>>>(a);
+  else if (sh.threads == 128) k_propagate<128, 6><<<sh.blocks, 128, 0, st>>>(a);
+  else return cudaErrorInvalidConfiguration;
   return cudaGetLastError();
 }
 
@@ -880,7 +897,7 @@ cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t
 
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local) {
   cudaFuncAttributes at;
-  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate);
+  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate<256, 3>);
   if (e != cudaSuccess) return e;
   *regs = at.numRegs;
   *max_threads = at.maxThreadsPerBlock;
@@ -891,8 +908,9 @@ cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size
 
 int propagate_max_blocks_per_sm(int threads) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate, threads, 0) != cudaSuccess) return 0;
-  return nb;
+  cudaError_t e = threads == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<128, 6>, 128, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<256, 3>, 256, 0);
+  return e == cudaSuccess ? nb : 0;
 }
 
 }  // namespace ppcb

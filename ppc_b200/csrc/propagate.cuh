@@ -37,6 +37,12 @@ struct KArgs {
   // options
   int deterministic;         // 1: photon i runs on thread i % threads (static order)
   uint32_t max_steps;        // 0: unlimited; else photons stopped after this many steps
+  int refill_below;          // photon pool: the warp also resamples when fewer than this are left
+  // batched launches (optional, all null otherwise)
+  const uint64_t* dyn;       // {num, nb} read by the kernel at start (graph replays)
+  const uint64_t* ev_off;    // per event: first slot of its hit region in `hits`
+  const uint32_t* ev_cap;    // per event: slots in its region
+  unsigned int* ev_cnt;      // per event: hits produced (may exceed ev_cap)
 };
 
 // Launch shape chosen by the host.
