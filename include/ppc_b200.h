@@ -79,6 +79,10 @@ int ppcb_destroy(ppcb_ctx* c);                                       /* stop(), 
 int ppcb_initialize(ppcb_ctx* c, const char* tables_dir, float enh); /* initialize(), gpu/ppc.cu:36; dir NULL: PPCTABLESDIR */
 int ppcb_choose(ppcb_ctx* c, int device);                            /* choose(), gpu/ppc.cu:490-508 */
 int ppcb_set_seed(ppcb_ctx* c, uint32_t seed);                       /* fixed seed instead of the clock (gpu/ini.cxx:792-795, DTMN) */
+/* deterministic: 0 photons taken dynamically (fastest); 1 photon i on thread i mod T, in the
+ * reference's order; 2 as 1 and each photon draws from its own stream keyed by (seed, i), so
+ * two runs that differ only in the ice share every photon's random numbers (common random
+ * numbers for finite differences and fits).  No counterpart in the reference. */
 int ppcb_set_options(ppcb_ctx* c, int deterministic, uint32_t max_steps, int blocks_per_sm);
 int ppcb_ini(ppcb_ctx* c);                                           /* ini(), gpu/ppc.cu:330-361 */
 int ppcb_fin(ppcb_ctx* c);                                           /* fin(), gpu/ppc.cu:398-402 */
@@ -180,6 +184,27 @@ int ppcb_batch_hits(ppcb_batch* b, ppcb_hit* out, uint64_t cap, uint64_t* n);
  * threshold) on a scaled-down copy of the batch and keeps the fastest for this context. */
 int ppcb_batch_autotune(ppcb_batch* b, const ppcb_bunch* bunches, int32_t nb, uint32_t events, uint64_t sample_photons,
                         ppcb_tune_info* out);
+
+/* ---- ice-model gradient ----
+ * No counterpart in the reference (llh/DirectFit fits the ice by repeated forward runs,
+ * llh/llh.cxx:1435-1634).  ppcb_set_ice replaces the per-layer scattering (be) and
+ * absorption (ba) coefficients at 400 nm (icemodel.dat columns 2-3, file order, `size`
+ * values each; NULL keeps) and rebuilds the wavelength table.  ppcb_gradient propagates
+ * the bunches once while recording each hit's provenance, then replays only the detected
+ * photons to form d/d be_j and d/d ba_j (FP64, file order) of
+ *   LL = sum_d (k_d log mu_d - mu_d)   with `observed` k_d (DOMs with mu_d = 0 left out), or
+ *   sum_d w_d mu_d                     with `weights` w_d when observed is NULL,
+ * where mu_d = scale x (simulated hits on DOM d).  Absorption terms are pathwise
+ * (-nr L_j dabs/dba), scattering terms score-function ((n_j/sca_j - L_j) dsca/dbe). */
+typedef struct ppcb_grad_info {
+  double ll;
+  uint64_t photons, hits, replayed, unmatched, steps;
+  double forward_ms, backward_ms;
+} ppcb_grad_info;
+int ppcb_set_ice(ppcb_ctx* c, const float* be, const float* ba);
+int ppcb_get_ice(ppcb_ctx* c, float* be, float* ba, int32_t* size);
+int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, const float* observed, const float* weights,
+                  double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba, ppcb_grad_info* info);
 
 /* ---- propagation that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device memory while

@@ -40,6 +40,12 @@ class TuneInfo(C.Structure):
                 ("pad_", C.c_int32), ("photons_per_s", C.c_double)]
 
 
+class GradInfo(C.Structure):
+    _fields_ = [("ll", C.c_double), ("photons", C.c_uint64), ("hits", C.c_uint64), ("replayed", C.c_uint64),
+                ("unmatched", C.c_uint64), ("steps", C.c_uint64), ("forward_ms", C.c_double),
+                ("backward_ms", C.c_double)]
+
+
 class Dom(C.Structure):
     _fields_ = [("R", C.c_float), ("F", C.c_float), ("r", C.c_float * 3)]
 
@@ -58,7 +64,7 @@ EXPORTS = [
     "ppcb_raw_copy", "ppcb_last_run", "ppcb_propagate", "ppcb_propagate_device", "ppcb_rng_get", "ppcb_rng_set",
     "ppcb_rng_reset", "ppcb_table", "ppcb_generate_device", "ppcb_index_probe_device", "ppcb_propagate_noalloc",
     "ppcb_batch_create", "ppcb_batch_destroy", "ppcb_batch_set_graph", "ppcb_batch_run", "ppcb_batch_counts",
-    "ppcb_batch_hits", "ppcb_batch_autotune",
+    "ppcb_batch_hits", "ppcb_batch_autotune", "ppcb_set_ice", "ppcb_get_ice", "ppcb_gradient",
 ]
 
 
@@ -116,6 +122,9 @@ def lib():
         "ppcb_batch_counts": (i32, [vp, vp, vp]),
         "ppcb_batch_hits": (i32, [vp, vp, u64, P(u64)]),
         "ppcb_batch_autotune": (i32, [vp, vp, i32, u32, u64, P(TuneInfo)]),
+        "ppcb_set_ice": (i32, [vp, vp, vp]),
+        "ppcb_get_ice": (i32, [vp, vp, vp, P(i32)]),
+        "ppcb_gradient": (i32, [vp, vp, i32, vp, vp, f64, u64, vp, vp, vp, P(GradInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -39,8 +39,12 @@ class PPC:
     def set_seed(self, seed):
         check(lib().ppcb_set_seed(self._c, int(seed) & 0xFFFFFFFF))
 
-    def set_options(self, deterministic=False, max_steps=1_000_000, blocks_per_sm=0):
-        check(lib().ppcb_set_options(self._c, int(bool(deterministic)), int(max_steps), int(blocks_per_sm)))
+    def set_options(self, deterministic=False, max_steps=1_000_000, blocks_per_sm=0, photon_streams=False):
+        """deterministic: photon i on thread i mod T (the reference's order).  photon_streams
+        (implies deterministic): each photon draws from its own stream keyed by (seed, i), so
+        runs that differ only in the ice share every photon's random numbers."""
+        mode = 2 if photon_streams else int(bool(deterministic))
+        check(lib().ppcb_set_options(self._c, mode, int(max_steps), int(blocks_per_sm)))
 
     def ini(self):
         check(lib().ppcb_ini(self._c))
@@ -260,3 +264,45 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _ice_methods():
+    def set_ice(self, be=None, ba=None):
+        """New per-layer be / ba at 400 nm (icemodel.dat columns 2-3, file order)."""
+        b = None if be is None else np.ascontiguousarray(be, np.float32)
+        a = None if ba is None else np.ascontiguousarray(ba, np.float32)
+        check(lib().ppcb_set_ice(self._c, _p(b), _p(a)))
+
+    def get_ice(self):
+        n = C.c_int32()
+        check(lib().ppcb_get_ice(self._c, None, None, C.byref(n)))
+        be = np.zeros(n.value, np.float32)
+        ba = np.zeros(n.value, np.float32)
+        check(lib().ppcb_get_ice(self._c, _p(be), _p(ba), C.byref(n)))
+        return be, ba
+
+    def gradient(self, bunches, observed=None, weights=None, scale=1.0, hit_cap=None):
+        """LL (or sum_d w_d mu_d) and its gradient in (be, ba), file order (ppcb_gradient)."""
+        from ._lib import GradInfo
+        bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
+        info_ = self.info()
+        gsize, size = info_["gsize"], info_["size"]
+        if hit_cap is None:
+            hit_cap = int(bunches["num"].sum() * 0.02) + (1 << 16)
+        obs = None if observed is None else np.ascontiguousarray(observed, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        counts = np.zeros(gsize, np.uint32)
+        g_be = np.zeros(size, np.float64)
+        g_ba = np.zeros(size, np.float64)
+        gi = GradInfo()
+        check(lib().ppcb_gradient(self._c, _p(bunches), len(bunches), _p(obs), _p(w), float(scale), int(hit_cap),
+                                  _p(counts), _p(g_be), _p(g_ba), C.byref(gi)))
+        return {"ll": gi.ll, "counts": counts, "g_be": g_be, "g_ba": g_ba,
+                "info": {k: getattr(gi, k) for k, _ in GradInfo._fields_}}
+
+    PPC.set_ice = set_ice
+    PPC.get_ice = get_ice
+    PPC.gradient = gradient
+
+
+_ice_methods()

@@ -68,7 +68,8 @@ int ppcb_set_seed(ppcb_ctx* c, uint32_t seed) {
 int ppcb_set_options(ppcb_ctx* c, int deterministic, uint32_t max_steps, int blocks_per_sm) {
   CTX_OR_FAIL(c);
   return guard([&] {
-    c->s.eng.deterministic = deterministic != 0;
+    if (deterministic < 0 || deterministic > 2) throw ppcb::Error("deterministic: 0, 1 or 2", PPCB_EARG);
+    c->s.eng.deterministic = deterministic;
     c->s.eng.max_steps = max_steps;
     c->s.eng.blocks_per_sm = blocks_per_sm;
   });

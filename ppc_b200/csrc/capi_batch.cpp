@@ -107,4 +107,43 @@ int ppcb_batch_autotune(ppcb_batch* x, const ppcb_bunch* bunches, int32_t nb, ui
   });
 }
 
+int ppcb_set_ice(ppcb_ctx* c, const float* be, const float* ba) {
+  if (!c) { ppcb_internal_set_error("null context"); return PPCB_EARG; }
+  return bguard([&] { c->s.eng.set_ice(be, ba); });
+}
+
+int ppcb_get_ice(ppcb_ctx* c, float* be, float* ba, int32_t* size) {
+  if (!c) { ppcb_internal_set_error("null context"); return PPCB_EARG; }
+  return bguard([&] {
+    const ppcb::Config& f = c->s.eng.cfg;
+    if (size) *size = f.p.size;
+    for (int j = 0; j < f.p.size; j++) {
+      if (be) be[j] = f.be[j];
+      if (ba) ba[j] = f.ba[j];
+    }
+  });
+}
+
+int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, const float* observed, const float* weights,
+                  double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba, ppcb_grad_info* info) {
+  if (!c || !bunches) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    ppcb::Engine::Grad r = c->s.eng.gradient(bunches, nb, observed, weights, scale, hit_cap);
+    const int size = c->s.eng.cfg.p.size;
+    if (counts) memcpy(counts, r.counts.data(), r.counts.size() * sizeof(uint32_t));
+    if (g_be) memcpy(g_be, r.g_be.data(), size * sizeof(double));
+    if (g_ba) memcpy(g_ba, r.g_ba.data(), size * sizeof(double));
+    if (info) {
+      info->ll = r.ll;
+      info->photons = r.photons;
+      info->hits = r.hits;
+      info->replayed = r.replayed;
+      info->unmatched = r.unmatched;
+      info->steps = r.steps;
+      info->forward_ms = r.forward_ms;
+      info->backward_ms = r.backward_ms;
+    }
+  });
+}
+
 }  // extern "C"

@@ -1,7 +1,7 @@
 // Configuration loader.  Each block names the part of gpu/ini.cxx it restates; the
 // arithmetic keeps the reference's float/double promotions so that the tables come
-// out bit-identical to the reference build on the same files (this file is compiled
-// with the reference's host flags, -O2 -ffast-math, gpu/Makefile:8,10).
+// out bit-identical to the reference's host code compiled the same way (IEEE float:
+// -O2 -ffp-contract=off, no fast-math, on both sides).
 #include "config.h"
 
 #include <sys/time.h>
@@ -213,6 +213,49 @@ void WaveGrid::read(WaveAcc& a, const std::vector<float>& qw, const std::vector<
       else { w2 = whi; f2 = 0; }
     }
     a.dat.push_back(wlo < w && w < whi ? (f1 * (w2 - w) + f2 * (w - w1)) / (w2 - w1) : 0);
+  }
+}
+
+// gpu/ini.cxx:1677-1691: absorption and scattering of wavelength bin n in every layer,
+// plus the derivatives the gradient needs: d sca / d be = l_a / (1 - g) and
+// d abs / d ba = D l_k (per wavelength; the same for every layer).
+void Config::fill_ice(int n, float wva) {
+  const float wv0 = 400;
+  const float a = ice_a, k = ice_k, A = ice_A, B = ice_B, D = ice_D, E = ice_E;
+  const int size = p.size;
+  float l_a = pow(wva / wv0, -a);
+  float l_k = pow(wva / wv0, -k);
+  float AB0 = A * exp(-B / wv0);
+  float ABl = A * exp(-B / wva);
+  for (int i = 0; i < size; i++) {
+    int j = size - 1 - i;
+    float bbl = bble > 0 ? dp[j] < bblz && dp[j] < bbly ? bble * (1 - dp[j] / bblz) * (1 - dp[j] / bbly) : 0 : 0;
+    float sca = (bbl + be[j] * l_a - rav[j] * p.sum * (srf + srw * l_a)) / (1 - p.g);
+    float abs = (D * ba[j] + E) * l_k + (ABl - arf * AB0 * l_k) * (1 + 0.01 * td[j]);
+    if (sca > 0 && abs > 0) {
+      absca[((size_t)n * size + i) * 2 + 0] = abs;
+      absca[((size_t)n * size + i) * 2 + 1] = sca;
+    } else throw Error("Invalid value of ice parameter, cannot proceed");
+  }
+  wgrad[n * 2 + 0] = l_a / (1 - p.g);
+  wgrad[n * 2 + 1] = D * l_k;
+}
+
+// New per-layer scattering (be) and absorption (ba) coefficients at 400 nm, file order
+// (icemodel.dat rows); null keeps the current values.  Rebuilds the per-wavelength table.
+void Config::set_ice(const float* be_new, const float* ba_new) {
+  const int size = p.size;
+  std::vector<float> be0 = be, ba0 = ba;
+  for (int j = 0; j < size; j++) {
+    if (be_new) be[j] = be_new[j];
+    if (ba_new) ba[j] = ba_new[j];
+  }
+  try {
+    for (int n = 0; n < PPCB_WNUM; n++) fill_ice(n, wvs[n].w);
+  } catch (...) {
+    be = be0; ba = ba0;
+    for (int n = 0; n < PPCB_WNUM; n++) fill_ice(n, wvs[n].w);
+    throw;
   }
 }
 
@@ -982,6 +1025,7 @@ void Config::load(const std::string& tables_dir) {
   wvs.assign(PPCB_WNUM, WaveSample());
   wmeta.assign(PPCB_WNUM, ppcb_wmeta());
   absca.assign((size_t)PPCB_WNUM * size * 2, 0.f);
+  wgrad.assign(PPCB_WNUM * 2, 0.f);
   for (int n = 0; n < PPCB_WNUM; n++) {
     float wvi = env.binf((n + 0.f) / PPCB_WNUM);
     int mi = std::min(std::max((int)floor(wvi), 0), qwv.num - 1);
@@ -1003,20 +1047,7 @@ void Config::load(const std::string& tables_dir) {
         mt.rat.push_back(rde);
       }
     }
-    float l_a = pow(wva / wv0, -a);
-    float l_k = pow(wva / wv0, -k);
-    float AB0 = A * exp(-B / wv0);
-    float ABl = A * exp(-B / wva);
-    for (int i = 0; i < size; i++) {
-      int j = size - 1 - i;
-      float bbl = bble > 0 ? dp[j] < bblz && dp[j] < bbly ? bble * (1 - dp[j] / bblz) * (1 - dp[j] / bbly) : 0 : 0;
-      float sca = (bbl + be[j] * l_a - rav[j] * p.sum * (srf + srw * l_a)) / (1 - p.g);
-      float abs = (D * ba[j] + E) * l_k + (ABl - arf * AB0 * l_k) * (1 + 0.01 * td[j]);
-      if (sca > 0 && abs > 0) {
-        absca[((size_t)n * size + i) * 2 + 0] = abs;
-        absca[((size_t)n * size + i) * 2 + 1] = sca;
-      } else throw Error("Invalid value of ice parameter, cannot proceed");
-    }
+    fill_ice(n, wva);
     float ng, npv = qwv.np(wva * 1.e-3, &ng);
     float c = 0.299792458;
     p.ocv = 1 / c;

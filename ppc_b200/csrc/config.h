@@ -106,6 +106,8 @@ class Config {
  public:
   // Loads everything.  `tables_dir` overrides PPCTABLESDIR when non-empty.
   void load(const std::string& tables_dir = "");
+  // New per-layer be / ba (icemodel.dat columns 2-3, file order; null keeps): rebuilds absca.
+  void set_ice(const float* be_new, const float* ba_new);
 
   // ---- kernel-facing tables (device image) ----
   ppcb_params p{};
@@ -121,6 +123,7 @@ class Config {
   std::vector<ppcb_dom> oms;               // [gsize]
   std::vector<uint32_t> rm;                // [rsize]
   std::vector<float> bfrt;                 // [(BFR_TAB+1)*4] birefringence functions of v = sqrt(1-|cos|)
+  std::vector<float> wgrad;                // [WNUM*2] d sca/d be, d abs/d ba per wavelength bin
 
   // ---- host-side tables ----
   std::vector<OMName> names;               // [gsize]
@@ -150,6 +153,7 @@ class Config {
   std::string ppcdir, omdir, icedir, tiltdir, holeice;
 
  private:
+  void fill_ice(int n, float wva);
   unsigned short sname(int n);
   std::map<int, unsigned short> sname_overflow_;
   unsigned short sname_next_ = 86 + 10 + 1;

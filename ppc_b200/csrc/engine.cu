@@ -216,7 +216,8 @@ KArgs Engine::args_for(int d) const {
   a.absca = g.absca; a.wmeta = g.wmeta; a.lp = g.lp; a.oms = g.oms; a.az = g.az; a.sc = g.sc;
   a.lr = g.lr; a.ls = g.ls; a.is = g.is; a.mcol = g.mcol; a.bfrt = g.bfrt;
   a.rs = g.rs; a.rm = g.rm;
-  a.deterministic = deterministic ? 1 : 0;
+  a.deterministic = deterministic;
+  a.seed = sv;
   a.max_steps = max_steps;
   a.refill_below = refill_below;
   return a;

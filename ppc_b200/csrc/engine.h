@@ -72,7 +72,7 @@ class Engine {
   ~Engine();
   Config cfg;
   unsigned int sv = 0;             // seed: MWC stream start and host rand_r state
-  bool deterministic = false;
+  int deterministic = 0;           // 0 dynamic photon order, 1 static order, 2 static + per-photon streams
   uint32_t max_steps = 1000000;     // per-photon step cap (typical photons take 20-100 steps)
   std::vector<DeviceCtx> devs;
   uint64_t pmax = 0, pmxo = 0;     // photons / bunches per launch
@@ -98,6 +98,22 @@ class Engine {
   void launch_device(int d, const ppcb_bunch* dbunch, const uint64_t* dbstart, int nb, uint64_t num,
                      ppcb_hit* dhits, uint64_t hcap, ppcb_ctrl* dctrl, cudaStream_t st);
   void reset_streams();            // re-seed every stream (reference rs_ini, gpu/ini.cxx:556-571)
+  // New per-layer be/ba (file order, null keeps): rebuilds and re-uploads the ice table.
+  void set_ice(const float* be, const float* ba);
+
+  struct Grad {
+    double ll = 0;                   // Poisson log-likelihood sum_d (k_d log mu_d - mu_d) over DOMs with mu_d > 0
+    std::vector<uint32_t> counts;    // simulated hits per DOM
+    std::vector<double> g_be, g_ba;  // d/d be_j, d/d ba_j in file order (icemodel.dat rows)
+    uint64_t photons = 0, hits = 0, replayed = 0, unmatched = 0, steps = 0;
+    float forward_ms = 0, backward_ms = 0;
+  };
+  // Gradient of sum_d w_d mu_d, mu_d = scale x (simulated hits on DOM d), with respect to the
+  // 2 x size ice coefficients.  With `observed` (per DOM) w_d = dLL/dmu_d of the Poisson
+  // log-likelihood; otherwise `weights` (per DOM) are used as given.  One recording
+  // forward launch over the bunches (device 0) and one replay of the recorded hits.
+  Grad gradient(const ppcb_bunch* b, int nb, const float* observed, const float* weights, double scale,
+                uint64_t hit_cap);
   double total_device_ms() const;
   KArgs args_for(int d) const;
 

@@ -1,0 +1,126 @@
+// Ice-model gradient (Engine::gradient, Engine::set_ice).  No counterpart in the reference:
+// llh/DirectFit fits the ice by repeated forward runs (llh/llh.cxx:1435-1634); here the
+// gradient of the likelihood with respect to all 2 x 171 per-layer coefficients comes from
+// one recording forward pass and a replay of the detected photons (propagate.cu, AdjHook).
+#include <cmath>
+
+#include "engine.h"
+
+namespace ppcb {
+
+void Engine::set_ice(const float* be, const float* ba) {
+  cfg.set_ice(be, ba);
+  if (!inited_) return;
+  for (auto& g : devs) {
+    check(cudaSetDevice(g.dev), "cudaSetDevice");
+    check(cudaMemcpy(g.absca, cfg.absca.data(), cfg.absca.size() * sizeof(float), cudaMemcpyHostToDevice),
+          "ice table");
+  }
+}
+
+namespace {
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  explicit DBuf(size_t n) { check(cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T)), "gradient buffer"); }
+  ~DBuf() { if (p) cudaFree(p); }
+};
+}  // namespace
+
+Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, const float* observed, const float* weights, double scale,
+                              uint64_t hit_cap) {
+  if (!inited_) throw Error("ini() must come before the gradient", 6);
+  if (nb <= 0) throw Error("no bunches", 7);
+  if (!observed && !weights) throw Error("gradient: observed counts or DOM weights required", 7);
+  DeviceCtx& g = devs[0];
+  check(cudaSetDevice(g.dev), "cudaSetDevice");
+  const int gsize = cfg.p.gsize, size = cfg.p.size;
+  std::vector<uint64_t> bs(nb + 1, 0);
+  for (int k = 0; k < nb; k++) bs[k + 1] = bs[k] + b[k].num;
+  DBuf<ppcb_bunch> db(nb);
+  DBuf<uint64_t> dbs(nb + 1);
+  DBuf<ppcb_hit> dh(hit_cap);
+  DBuf<unsigned char> dprov(hit_cap * kProvBytes);
+  DBuf<ppcb_ctrl> dctrl(1);
+  DBuf<unsigned int> dcnt(gsize);
+  DBuf<float> dw(gsize);
+  DBuf<float2> dwg(PPCB_WNUM);
+  DBuf<double> dgo(2 * PPCB_MAXLYS);
+  DBuf<unsigned int> dstat(2);
+  cudaStream_t st = g.st;
+  check(cudaMemcpyAsync(db.p, b, nb * sizeof(ppcb_bunch), cudaMemcpyHostToDevice, st), "H2D bunches");
+  check(cudaMemcpyAsync(dbs.p, bs.data(), (nb + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "H2D offsets");
+  check(cudaMemcpyAsync(dwg.p, cfg.wgrad.data(), PPCB_WNUM * sizeof(float2), cudaMemcpyHostToDevice, st), "H2D");
+  check(cudaMemsetAsync(dctrl.p, 0, sizeof(ppcb_ctrl), st), "memset");
+  check(cudaMemsetAsync(dcnt.p, 0, gsize * sizeof(unsigned int), st), "memset");
+  check(cudaMemsetAsync(dgo.p, 0, 2 * PPCB_MAXLYS * sizeof(double), st), "memset");
+  check(cudaMemsetAsync(dstat.p, 0, 2 * sizeof(unsigned int), st), "memset");
+  cudaEvent_t e0, e1, e2;
+  check(cudaEventCreate(&e0), "event");
+  check(cudaEventCreate(&e1), "event");
+  check(cudaEventCreate(&e2), "event");
+  // recording forward pass
+  KArgs a = args_for(0);
+  a.bunches = db.p; a.bstart = dbs.p; a.nb = nb; a.num = bs[nb];
+  a.hits = dh.p; a.hcap = hit_cap; a.ctrl = dctrl.p; a.prov = dprov.p;
+  check(cudaEventRecord(e0, st), "event");
+  const int rec_blocks = g.shape.threads == 256 ? g.shape.blocks : g.shape.blocks * g.shape.threads / 256;
+  check(launch_propagate(a, LaunchShape{rec_blocks, 256}, st), "recording launch");
+  check(cudaEventRecord(e1, st), "event");
+  ppcb_ctrl c;
+  check(cudaMemcpyAsync(&c, dctrl.p, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H ctrl");
+  check(cudaStreamSynchronize(st), "recording pass");
+  const uint64_t nh = std::min<uint64_t>(c.hidx, hit_cap);
+  if (c.hidx > hit_cap) throw Error("gradient: hit capacity too small (" + std::to_string(c.hidx) + " hits)", 7);
+  check(launch_dom_hist(dh.p, nh, dcnt.p, st), "histogram");
+  Grad out;
+  out.counts.resize(gsize);
+  check(cudaMemcpyAsync(out.counts.data(), dcnt.p, gsize * sizeof(unsigned int), cudaMemcpyDeviceToHost, st), "D2H");
+  check(cudaStreamSynchronize(st), "histogram");
+  // per-DOM weights: dLL/dmu_d = k_d/mu_d - 1 (times d mu_d / d count = scale)
+  std::vector<float> w(gsize, 0.f);
+  double ll = 0;
+  for (int d = 0; d < gsize; d++) {
+    const double mu = scale * out.counts[d];
+    if (observed) {
+      if (mu > 0) {
+        ll += observed[d] * std::log(mu) - mu;
+        w[d] = (float)(scale * (observed[d] / mu - 1.0));
+      }
+    } else w[d] = (float)(scale * weights[d]);
+  }
+  out.ll = ll;
+  check(cudaMemcpyAsync(dw.p, w.data(), gsize * sizeof(float), cudaMemcpyHostToDevice, st), "H2D weights");
+  // replay of the detected photons
+  KArgs r = args_for(0);
+  r.ctrl = dctrl.p;
+  check(launch_adjoint(r, dh.p, dprov.p, nh, dw.p, dwg.p, dgo.p, dstat.p, g.prop.multiProcessorCount * 4, st),
+        "replay launch");
+  check(cudaEventRecord(e2, st), "event");
+  std::vector<double> go(2 * PPCB_MAXLYS);
+  unsigned int stat[2];
+  check(cudaMemcpyAsync(go.data(), dgo.p, go.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H gradient");
+  check(cudaMemcpyAsync(stat, dstat.p, sizeof(stat), cudaMemcpyDeviceToHost, st), "D2H stats");
+  check(cudaStreamSynchronize(st), "replay");
+  check(cudaEventElapsedTime(&out.forward_ms, e0, e1), "elapsed");
+  check(cudaEventElapsedTime(&out.backward_ms, e1, e2), "elapsed");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  // kernel layers run from the deepest row of icemodel.dat (layer i <-> row size-1-i)
+  out.g_be.assign(size, 0.0);
+  out.g_ba.assign(size, 0.0);
+  for (int i = 0; i < size; i++) {
+    out.g_be[size - 1 - i] = go[i];
+    out.g_ba[size - 1 - i] = go[PPCB_MAXLYS + i];
+  }
+  out.photons = bs[nb];
+  out.hits = nh;
+  out.steps = c.steps;
+  out.replayed = stat[0];
+  out.unmatched = stat[1];
+  g.device_ms += out.forward_ms + out.backward_ms;
+  return out;
+}
+
+}  // namespace ppcb

@@ -21,6 +21,8 @@
 //     same fast-math intrinsics as the reference's GPU build (--use_fast_math).
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "propagate.cuh"
 #include "tilt.h"
 
@@ -63,6 +65,19 @@ __device__ __forceinline__ float xrnd(Rng& s) {
   s.x = (uint32_t)sda;
   s.y = (uint32_t)(sda >> 32);
   return 2.f - __uint_as_float((s.x >> 9) | 0x3f800000u);
+}
+
+// Per-photon stream (no counterpart in the reference): the MWC state of photon i is a
+// SplitMix64 hash (Steele, Lea, Flood, OOPSLA 2014) of (seed, i), the carry mapped into
+// [0, a) of the thread's multiplier; the photon's random numbers then depend only on
+// (seed, i, thread multiplier) and not on what the thread simulated before.
+__device__ __forceinline__ void photon_stream(Rng& s, uint64_t i, uint32_t seed) {
+  uint64_t z = ((uint64_t)seed << 32 | 0x2545f491u) + (i + 1) * 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  z ^= z >> 31;
+  s.x = (uint32_t)z;
+  s.y = __umulhi((uint32_t)(z >> 32), s.a);
 }
 
 // gpu/pro.cu:59-85
@@ -214,6 +229,7 @@ struct Photon {
   int ofla;        // DOM that absorbs without registering (flasher), or <-1 veto code
   int om0;         // flasher DOM on the first step, -1 afterwards
   uint32_t steps;
+  int nhit;        // hits registered so far (ordinal of the next one)
 };
 
 __device__ __forceinline__ int find_bunch(const KArgs& a, int nb, uint64_t i, int hint) {
@@ -354,7 +370,7 @@ __device__ __forceinline__ void generate(const KArgs& a, const ppcb_bunch& p, Rn
 
 __device__ __forceinline__ float2 ice(const float2* __restrict__ t, int J) { return __ldg(&t[J]); }
 
-__device__ __forceinline__ void emit_hit(const KArgs& a, const ppcb_hit& h) {
+__device__ __forceinline__ unsigned long long emit_hit(const KArgs& a, const ppcb_hit& h) {
   if (a.ev_cnt) {  // batched launch: the event's own region, sized from an upper bound
     const unsigned int e = h.n;
     const unsigned int slot = atomicAdd(&a.ev_cnt[e], 1u);
@@ -364,7 +380,7 @@ __device__ __forceinline__ void emit_hit(const KArgs& a, const ppcb_hit& h) {
       dst[0] = src[0];
       dst[1] = src[1];
     }
-    return;
+    return ~0ull;
   }
   cg::coalesced_group g = cg::coalesced_threads();
   unsigned long long base = 0;
@@ -376,12 +392,95 @@ __device__ __forceinline__ void emit_hit(const KArgs& a, const ppcb_hit& h) {
     dst[0] = src[0];
     dst[1] = src[1];
   }
+  return base;
 }
+
+// ---------------------------------------------------------------- step hooks
+// The plain propagation: hits are appended, nothing else is observed.
+struct NoHook {
+  __device__ __forceinline__ bool active() const { return false; }
+  __device__ __forceinline__ void segment(int, float, int, float, float, float, float, float, int) {}
+  __device__ __forceinline__ void scatter(int, float) {}
+  __device__ __forceinline__ void hit(const KArgs& a, const ppcb_hit& h, Photon&) { emit_hit(a, h); }
+};
+
+// Provenance of a hit, enough to replay its photon: the sampled photon, the stream state
+// of the propagating thread before its first draw, that thread, and the hit's ordinal
+// among the photon's hits.  64 bytes, stored at the hit's slot.
+struct Prov {
+  float4 r, n;
+  int4 m;    // wavelength bin, segment, flasher DOM, veto code
+  uint4 s;   // stream x, stream y, thread, hit ordinal
+};
+
+// Gradient hook.  In the recording forward pass it writes each hit's provenance; in the
+// replay it accumulates, for the photon's path up to the recorded hit, the derivatives of
+// that hit's weight with respect to the per-layer scattering (be) and absorption (ba)
+// coefficients of the ice model:
+//   absorption (pathwise): d/dba_j = -D l_k(lambda) nr L_j      (survival exp(-sum abs nr L))
+//   scattering (score):    d/dbe_j = l_a(lambda)/(1-g) (n_j/sca_j - L_j)
+// with L_j the path length in layer j (split as the reference splits overburdens,
+// gpu/pro.cu:678-696) and n_j the scatterings in layer j.  Sums go to FP64 shared memory.
+struct AdjHook {
+  bool replay;
+  int target;          // replay: ordinal of the hit to stop at
+  uint32_t target_i;   // replay: its DOM
+  float target_t;      // replay: its time
+  bool done, matched;
+  float w_be, w_ba;    // hit weight x dsca/dbe, x dabs/dba (per wavelength)
+  double* g_be;
+  double* g_ba;
+  Prov* prov_out;      // recording: provenance array, indexed like the hits
+  Prov start;          // recording: this thread's current photon
+  __device__ __forceinline__ bool active() const { return replay && !done; }
+  // path length `del` from layer coordinate z (layer I), direction sign/anz, layer step edh.
+  // The hook's arithmetic is in explicitly rounded intrinsics, which the compiler neither
+  // contracts nor shares with the step's own expressions: the step compiles to the same
+  // floating-point operations whether the hook is live (replay) or not (recording).
+  __device__ __forceinline__ void segment(int I, float z, int sign, float anz, float edh, float nr, float del,
+                                          float nz, int size) {
+    if (!active() || !(del > 0)) return;
+    const float y = __fadd_rn(z, __fdiv_rn(__fmul_rn(nz, del), edh));
+    const int J = min(max(__float2int_rn(y), 0), size - 1);
+    if (I == J) { add(I, del, nr); return; }
+    const float f = __fdiv_rn(edh, anz);
+    const float s = (float)sign;
+    add(I, __fmul_rn(__fsub_rn(0.5f, __fmul_rn(s, __fsub_rn(z, (float)I))), f), nr);
+    add(J, __fmul_rn(__fadd_rn(0.5f, __fmul_rn(s, __fsub_rn(y, (float)J))), f), nr);
+    for (int i = I + sign; i != J && (unsigned)i < (unsigned)size; i += sign) add(i, f, nr);
+  }
+  __device__ __forceinline__ void add(int j, float len, float nr) {
+    if (!(len > 0)) return;
+    atomicAdd(&g_be[j], -(double)w_be * len);
+    atomicAdd(&g_ba[j], -(double)w_ba * nr * len);
+  }
+  __device__ __forceinline__ void scatter(int J, float scaJ) {
+    if (active()) atomicAdd(&g_be[J], (double)w_be / scaJ);
+  }
+  __device__ __forceinline__ void hit(const KArgs& a, const ppcb_hit& h, Photon& ph) {
+    if (replay) {
+      if (!done && ph.nhit == target) {
+        done = true;
+        matched = h.i == target_i && __float_as_uint(h.t) == __float_as_uint(target_t);
+      }
+      ph.nhit++;
+      return;
+    }
+    const unsigned long long slot = emit_hit(a, h);
+    if (prov_out && slot < a.hcap) {
+      Prov p = start;
+      p.s.w = (unsigned)ph.nhit;
+      prov_out[slot] = p;
+    }
+    ph.nhit++;
+  }
+};
 
 // gpu/pro.cu:499-888: one propagation step (one scattering segment).  Returns with
 // ph.TOT == 0 once the photon is absorbed or registered.
+template <class HOOK>
 __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon& ph, Rng& s,
-                                     unsigned int& nan_steps) {
+                                     unsigned int& nan_steps, HOOK& hk) {
   const ppcb_params& e = a.p;
   const float2* __restrict__ wz = a.absca + (size_t)ph.wl * e.size;
   float4 r = ph.r, n = ph.n;
@@ -554,6 +653,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
     }
   } else { SCA = 0; TOT = tot * nr; }
 
+  hk.segment(I, z, sign, anz, edh, nr, fin, n.z, e.size);  // bulk-ice part of the step (the rest is hole ice)
   r.x += del * n.x; r.y += del * n.y; r.z += del * n.z; r.w += del * n.w;
 
   if (!isfinite(TOT) || !isfinite(SCA)) {  // gpu/pro.cu:728
@@ -576,7 +676,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
       float dz = dom.r[2] - r.z + sqd * n.z;
       h.dth = acosf(fminf(fmaxf(dz / (e.xR * dom.R * dom.F), -1.f), 1.f));
       h.dph = atan2f(dy, dx);
-      emit_hit(a, h);
+      hk.hit(a, h, ph);
       if (e.xR == 1) TOT = 0;
       else ph.old = om;
     }
@@ -654,6 +754,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
       normalize3(n);
     }
     if (SCA < XXX) {  // scattering, gpu/pro.cu:838-887
+      if (!hole) hk.scatter(J, ice(wz, J).y);
       SCA = 0;
       float sf, g, gr;
       if (hole) { sf = e.SF; g = e.G; gr = e.GR; }
@@ -722,7 +823,7 @@ struct PhotonPool {
   int count;
 };
 
-template <int BLOCK, int MINB>
+template <int BLOCK, int MINB, bool REC>
 __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant__ KArgs a) {
   __shared__ SmemTables S;
   __shared__ PhotonPool pools[BLOCK / 32];
@@ -748,6 +849,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
   int hint = 0;
   unsigned long long nsteps = 0;
   unsigned int nan_steps = 0, capped = 0;
+  // REC: the gradient's recording pass (same step code as the replay, see AdjHook)
+  typename std::conditional<REC, AdjHook, NoHook>::type hk;
+  if constexpr (REC) {
+    hk.replay = false;
+    hk.done = false;
+    hk.prov_out = static_cast<Prov*>(a.prov);
+  }
   // every lane of the warp stays in this loop until the warp is done, so the warp-wide
   // operations below always see all 32 lanes
   while (true) {
@@ -772,6 +880,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       }
       Photon g;
       if (gen) {
+        if (a.deterministic == 2) photon_stream(s, gidx, a.seed);
         hint = find_bunch(a, nb, gidx, hint);
         const ppcb_bunch p = a.bunches[hint];
         generate(a, p, s, g);
@@ -802,6 +911,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
         __syncwarp();
       }
       if (alive && (dead >> lane & 1u)) {  // a fresh photon: absorption depth, gpu/pro.cu:496-497
+        ph.nhit = 0;
+        if constexpr (REC) {
+          hk.start.r = ph.r;
+          hk.start.n = ph.n;
+          hk.start.m = make_int4(ph.wl, (int)ph.niw, ph.om0, ph.ofla);
+          hk.start.s = make_uint4(s.x, s.y, gt, 0);
+        }
         ph.TOT = -logf(xrnd(s));
         ph.SCA = 0;
         ph.old = -1;
@@ -814,7 +930,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       continue;
     }
     if (alive) {
-      step(a, S, ph, s, nan_steps);
+      step(a, S, ph, s, nan_steps, hk);
       ph.steps++;
       nsteps++;
       if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) { ph.TOT = 0; capped++; }
@@ -824,6 +940,84 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
   a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
   atomicAdd(&a.ctrl->steps, nsteps);
   if (capped) atomicAdd(&a.ctrl->capped, capped);
+}
+
+// Gradient replay: one thread per recorded hit.  The photon is restarted from its
+// provenance (sampled state, stream state, thread multiplier) and stepped with the same
+// step<AdjHook> code as the recording pass, so it retraces the same path; the hook sums
+// the path's per-layer derivative terms, weighted by the hit's DOM weight, until the
+// recorded hit is reached again.  A replay that does not end on the recorded hit (same
+// DOM, same time bits) is counted in stats[1].
+__global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a, const ppcb_hit* __restrict__ hits,
+                                                 const Prov* __restrict__ prov, uint64_t nh,
+                                                 const float* __restrict__ wdom, const float2* __restrict__ wgrad,
+                                                 double* g_out, unsigned int* stats) {
+  __shared__ SmemTables S;
+  __shared__ double gbe[PPCB_MAXLYS], gba[PPCB_MAXLYS];
+  for (int i = threadIdx.x; i < PPCB_MAXLYS; i += blockDim.x) { gbe[i] = 0; gba[i] = 0; }
+  load_tables(a, S);
+  unsigned int nan_steps = 0, replayed = 0, unmatched = 0;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x) {
+    const ppcb_hit h = hits[k];
+    const float w = wdom[h.i];
+    if (w == 0) continue;
+    const Prov P = prov[k];
+    Rng s;
+    s.x = P.s.x; s.y = P.s.y; s.a = a.rm[P.s.z];
+    Photon ph;
+    ph.r = P.r; ph.n = P.n;
+    ph.wl = P.m.x; ph.niw = (uint32_t)P.m.y; ph.om0 = P.m.z; ph.ofla = P.m.w;
+    ph.nhit = 0;
+    ph.TOT = -logf(xrnd(s));  // as at pick-up in the recording pass
+    ph.SCA = 0;
+    ph.old = -1;
+    ph.steps = 0;
+    if (ph.ofla < -1) ph.TOT = 0;
+    AdjHook hk;
+    hk.replay = true;
+    hk.target = (int)P.s.w;
+    hk.target_i = h.i;
+    hk.target_t = h.t;
+    hk.done = false;
+    hk.matched = false;
+    const float2 c = wgrad[ph.wl];
+    hk.w_be = w * c.x;
+    hk.w_ba = w * c.y;
+    hk.g_be = gbe;
+    hk.g_ba = gba;
+    hk.prov_out = nullptr;
+    while (!hk.done && ph.TOT != 0 && ph.steps < a.max_steps) {
+      step(a, S, ph, s, nan_steps, hk);
+      ph.steps++;
+    }
+    replayed++;
+    if (!hk.matched) unmatched++;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < a.p.size; i += blockDim.x) {
+    if (gbe[i] != 0) atomicAdd(&g_out[i], gbe[i]);
+    if (gba[i] != 0) atomicAdd(&g_out[PPCB_MAXLYS + i], gba[i]);
+  }
+  if (replayed) atomicAdd(&stats[0], replayed);
+  if (unmatched) atomicAdd(&stats[1], unmatched);
+}
+
+__global__ void k_dom_hist(const ppcb_hit* __restrict__ hits, uint64_t nh, unsigned int* counts) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(&counts[hits[k].i], 1u);
+}
+
+cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, const float* wdom,
+                           const float2* wgrad, double* g_out, unsigned int* stats, int blocks, cudaStream_t st) {
+  if (nh == 0) return cudaSuccess;
+  k_adjoint<<<blocks, 256, 0, st>>>(a, hits, static_cast<const Prov*>(prov), nh, wdom, wgrad, g_out, stats);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, cudaStream_t st) {
+  if (nh == 0) return cudaSuccess;
+  k_dom_hist<<<592, 256, 0, st>>>(hits, nh, counts);
+  return cudaGetLastError();
 }
 
 // Phase-1 only: thread t samples photon t with stream t (test entry point).
@@ -875,8 +1069,11 @@ __global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos
 // Two compiled shapes: 256 threads x 3 blocks per SM and 128 x 6 (the same 768 threads
 // per SM at <= 80 registers); the autotuner picks one.
 cudaError_t launch_propagate(const KArgs& a, LaunchShape sh, cudaStream_t st) {
-  if (sh.threads == 256) k_propagate<256, 3><<<sh.blocks, 256, 0, st>>>(a);
-  else if (sh.threads == 128) k_propagate<128, 6><<<sh.blocks, 128, 0, st>>>(a);
+  if (a.prov) {  // the gradient's recording pass
+    if (sh.threads != 256) return cudaErrorInvalidConfiguration;
+    k_propagate<256, 3, true><<<sh.blocks, 256, 0, st>>>(a);
+  } else if (sh.threads == 256) k_propagate<256, 3, false><<<sh.blocks, 256, 0, st>>>(a);
+  else if (sh.threads == 128) k_propagate<128, 6, false><<<sh.blocks, 128, 0, st>>>(a);
   else return cudaErrorInvalidConfiguration;
   return cudaGetLastError();
 }
@@ -897,7 +1094,7 @@ cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t
 
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local) {
   cudaFuncAttributes at;
-  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate<256, 3>);
+  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate<256, 3, false>);
   if (e != cudaSuccess) return e;
   *regs = at.numRegs;
   *max_threads = at.maxThreadsPerBlock;
@@ -908,8 +1105,8 @@ cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size
 
 int propagate_max_blocks_per_sm(int threads) {
   int nb = 0;
-  cudaError_t e = threads == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<128, 6>, 128, 0)
-                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<256, 3>, 256, 0);
+  cudaError_t e = threads == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<128, 6, false>, 128, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<256, 3, false>, 256, 0);
   return e == cudaSuccess ? nb : 0;
 }
 

@@ -35,7 +35,9 @@ struct KArgs {
   uint64_t hcap;
   ppcb_ctrl* ctrl;
   // options
-  int deterministic;         // 1: photon i runs on thread i % threads (static order)
+  int deterministic;         // 1: photon i runs on thread i % threads (static order);
+                             // 2: as 1, and photon i draws from its own stream (seed, i)
+  uint32_t seed;             // stream seed of mode 2
   uint32_t max_steps;        // 0: unlimited; else photons stopped after this many steps
   int refill_below;          // photon pool: the warp also resamples when fewer than this are left
   // batched launches (optional, all null otherwise)
@@ -43,6 +45,8 @@ struct KArgs {
   const uint64_t* ev_off;    // per event: first slot of its hit region in `hits`
   const uint32_t* ev_cap;    // per event: slots in its region
   unsigned int* ev_cnt;      // per event: hits produced (may exceed ev_cap)
+  // gradient (optional): recording pass writes 64-byte provenance records here, one per hit slot
+  void* prov;
 };
 
 // Launch shape chosen by the host.
@@ -56,6 +60,10 @@ cudaError_t launch_propagate(const KArgs& a, LaunchShape s, cudaStream_t st);
 cudaError_t launch_generate(const KArgs& a, LaunchShape s, void* pbuf_out, cudaStream_t st);
 cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t* out_i, float* out_f,
                                cudaStream_t st);
+cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, const float* wdom,
+                           const float2* wgrad, double* g_out, unsigned int* stats, int blocks, cudaStream_t st);
+cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, cudaStream_t st);
+constexpr size_t kProvBytes = 64;  // provenance record per hit slot of the gradient's recording pass
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local);
 int propagate_max_blocks_per_sm(int threads);
 

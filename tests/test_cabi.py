@@ -114,6 +114,29 @@ def test_corrupt_ice_table_is_rejected(tmp_path, ice_small):
     c.close()
 
 
+def test_ice_coefficients_round_trip_and_reject_bad_values(ice_small):
+    """ppcb_get_ice / ppcb_set_ice on the host table (no device needed before ini)."""
+    rows = np.loadtxt(os.path.join(ice_small, "icemodel.dat"))
+    c = PPC()
+    c.initialize(1.0, ice_small)
+    be, ba = c.get_ice()
+    assert np.allclose(be, rows[:, 1].astype(np.float32)) and np.allclose(ba, rows[:, 2].astype(np.float32))
+    before = c.table("absca")
+    c.set_ice(be * 1.5, None)
+    be2, ba2 = c.get_ice()
+    assert np.allclose(be2, be * 1.5) and np.array_equal(ba2, ba)
+    assert c.table("absca") != before
+    bad = ba.copy()
+    bad[3] = -1.0
+    with pytest.raises(PPCError) as e:
+        c.set_ice(None, bad)
+    assert "Invalid value of ice parameter" in str(e.value)
+    assert np.array_equal(c.get_ice()[1], ba)  # restored
+    c.set_options(photon_streams=True)
+    assert _lib.lib().ppcb_set_options(c._c, 3, 0, 0) == 7  # PPCB_EARG
+    c.close()
+
+
 def test_propagation_before_ini_is_an_error(ice_small):
     c = PPC()
     c.initialize(1.0, ice_small)
