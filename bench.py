@@ -353,13 +353,16 @@ def run_ours(args, rank, world, local):
     e2e_value = world * photons * args.steps / e2e_total
     launch_ms = total_ms / args.steps
     steps_per_launch = steps_done / args.steps
-    # roofline: FP32 issue.  Algorithmic FP32 operations per photon-step (measured with
-    # ncu on this kernel, thread-level FADD+FMUL+FFMA(x2), profiles/propagate_fp32_ops.md)
+    # roofline: FP32.  FP32 operations per photon-step (thread-level FADD + FMUL + 2 x FFMA,
+    # counted by ncu on this kernel, profiles/k_propagate_cascade.md) x photon-steps of the
+    # launch / its event-timed duration, against the FFMA throughput measured on this GPU
+    # by the library's own FFMA loop (ppcb_fp32_peak).
+    from ppc_b200.api import fp32_peak
     ops_per_step = args.fp32_ops_per_step
     achieved = ops_per_step * steps_per_launch / (launch_ms / 1000.0) / 1e12
     props = torch.cuda.get_device_properties(local)
-    sm_max = (clocks or {}).get("sm_max_mhz") or 1965.0
-    peak = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
+    peak = fp32_peak(local, repeats=5)
+    traffic = args.dram_bytes_per_step * steps_per_launch
     h2d = 64 + 16
     d2h = 32 * (e2e_hits / max(1, args.steps)) + 56
     line = {
@@ -376,10 +379,14 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h), "gpu_launches": args.steps},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "peak_source": f"nominal FP32 issue: {props.multi_processor_count} SMs x 128 lanes x 2 flop x "
-                                    f"{sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
-                     "ops_per_photon_step": ops_per_step},
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"measured: FFMA loop on all {props.multi_processor_count} SMs (ppcb_fp32_peak); "
+                                    "no FP32 figure is among the driver-measured peaks",
+                     "ops_per_photon_step": ops_per_step,
+                     "traffic_source": f"ncu dram__bytes_read+write per photon-step ({args.dram_bytes_per_step:.1f} B) "
+                                       "on a 1e7-photon launch, scaled by this launch's photon-steps",
+                     "hbm": {"achieved_gbs": traffic / (launch_ms / 1000.0) / 1e9,
+                             "peak_gbs": _peaks().get("hbm_gbs"), "peak_source": "of measured (MEASURED_PEAKS.json)"}},
         "clocks": clocks,
     }
     if not args.no_plain_kernel:
@@ -410,7 +417,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--photons", type=int, default=PHOTONS)
     ap.add_argument("--ref-photons", type=int, default=200_000)
-    ap.add_argument("--fp32-ops-per-step", type=float, default=250.0)
+    ap.add_argument("--fp32-ops-per-step", type=float, default=405.5)
+    ap.add_argument("--dram-bytes-per-step", type=float, default=0.007)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")

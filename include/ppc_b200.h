@@ -223,6 +223,12 @@ int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, const floa
 int ppcb_propagate_noalloc(ppcb_ctx* c, int device, const ppcb_bunch* bunches, int32_t nb, uint64_t num,
                            ppcb_hit* hits, uint64_t hcap, uint64_t* nhits, void* stream);
 
+/* ---- measurement ----
+ * No counterpart in the reference.  FP32 FMA throughput of `device` (TFLOP/s, best of
+ * `repeats` launches of an FFMA loop over every SM): the denominator of the propagation
+ * kernel's FP32 roofline. */
+int ppcb_fp32_peak(int device, int repeats, double* tflops, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -306,3 +306,10 @@ def _ice_methods():
 
 
 _ice_methods()
+
+
+def fp32_peak(device=0, repeats=5):
+    """Measured FP32 FMA throughput of `device` in TFLOP/s (ppcb_fp32_peak)."""
+    t, ms = C.c_double(), C.c_double()
+    check(lib().ppcb_fp32_peak(int(device), int(repeats), C.byref(t), C.byref(ms)))
+    return t.value
