@@ -368,6 +368,41 @@ __device__ __forceinline__ void generate(const KArgs& a, const ppcb_bunch& p, Rn
   ph.wl = j; ph.niw = p.q; ph.om0 = fla; ph.ofla = ofla;
 }
 
+// The two rare branches of the photon loop, sampling (once per photon) and the hit record
+// (about once per 2e4 steps), are compiled out of line: inlined, their code (source
+// types, Cherenkov cone, acos/atan2) would share the instruction cache with the step.
+struct Sampled {
+  Photon ph;
+  uint32_t x, y;  // stream state after the draws
+};
+
+__device__ __noinline__ Sampled sample_photon(const KArgs& a, int bunch, uint32_t sx, uint32_t sy, uint32_t sa) {
+  Rng s;
+  s.x = sx; s.y = sy; s.a = sa;
+  Sampled out;
+  const ppcb_bunch p = a.bunches[bunch];
+  generate(a, p, s, out.ph);
+  out.x = s.x; out.y = s.y;
+  return out;
+}
+
+// gpu/pro.cu:734-745: the hit record (photon and DOM-surface angles)
+__device__ __noinline__ ppcb_hit hit_record(const KArgs& a, int om, float4 r, float4 n, float sqd, uint32_t niw,
+                                           int wl) {
+  const ppcb_params& e = a.p;
+  ppcb_hit h;
+  h.i = om; h.t = r.w; h.n = niw; h.z = a.wmeta[wl].wvl;
+  h.pth = acosf(n.z); h.pph = atan2f(n.y, n.x);
+  sqd *= e.xR - 1;
+  const ppcb_dom dom = a.oms[om];
+  float dx = dom.r[0] - r.x + sqd * n.x;
+  float dy = dom.r[1] - r.y + sqd * n.y;
+  float dz = dom.r[2] - r.z + sqd * n.z;
+  h.dth = acosf(fminf(fmaxf(dz / (e.xR * dom.R * dom.F), -1.f), 1.f));
+  h.dph = atan2f(dy, dx);
+  return h;
+}
+
 __device__ __forceinline__ float2 ice(const float2* __restrict__ t, int J) { return __ldg(&t[J]); }
 
 __device__ __forceinline__ unsigned long long emit_hit(const KArgs& a, const ppcb_hit& h) {
@@ -666,16 +701,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
   if (om != -1) {  // DOM hit, gpu/pro.cu:731-753
     if (om == ph.ofla) TOT = 0;
     else {
-      ppcb_hit h;
-      h.i = om; h.t = r.w; h.n = ph.niw; h.z = a.wmeta[ph.wl].wvl;
-      h.pth = acosf(n.z); h.pph = atan2f(n.y, n.x);
-      sqd *= e.xR - 1;
-      const ppcb_dom dom = a.oms[om];
-      float dx = dom.r[0] - r.x + sqd * n.x;
-      float dy = dom.r[1] - r.y + sqd * n.y;
-      float dz = dom.r[2] - r.z + sqd * n.z;
-      h.dth = acosf(fminf(fmaxf(dz / (e.xR * dom.R * dom.F), -1.f), 1.f));
-      h.dph = atan2f(dy, dx);
+      const ppcb_hit h = hit_record(a, om, r, n, sqd, ph.niw, ph.wl);
       hk.hit(a, h, ph);
       if (e.xR == 1) TOT = 0;
       else ph.old = om;
@@ -882,8 +908,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       if (gen) {
         if (a.deterministic == 2) photon_stream(s, gidx, a.seed);
         hint = find_bunch(a, nb, gidx, hint);
-        const ppcb_bunch p = a.bunches[hint];
-        generate(a, p, s, g);
+        const Sampled smp = sample_photon(a, hint, s.x, s.y, s.a);
+        g = smp.ph;
+        s.x = smp.x; s.y = smp.y;
       }
       if (a.deterministic) {
         if (gen) { ph = g; alive = true; }

@@ -87,6 +87,42 @@ def test_index_helpers_bit_exact(kind, request):
     c.close()
 
 
+@pytest.mark.parametrize("kind", ["small_tilt", "full"])
+def test_layer_lookup_near_rounding_boundaries(kind, request):
+    """Positions moved to within +-1e-2 layer units of a rounding boundary of the layer
+    index (down to a few ulps): the layer the CUDA lookup returns is the oracle's."""
+    ice = request.getfixturevalue("ice_" + kind)
+    c = _ctx(ice)
+    tb = O.tables_from_product(c)
+    p = c.params()
+    rng = np.random.default_rng(12)
+    pos = _random_probe_points(50000, rng, zr=(-480, 480))
+    f32 = np.float32
+    off = rng.choice(np.array([-1e-2, -1e-3, -2e-4, -1e-5, 0.0, 1e-5, 2e-4, 1e-3, 1e-2], np.float32), len(pos))
+    target = None
+    for _ in range(6):  # the tilt shift depends on depth: move z onto its target iteratively
+        ri, rf = O.index_probe(tb, pos)
+        z = ((pos[:, 2] - rf[:, 0]) - f32(p.hmin)) * f32(p.rdh)
+        if target is None:
+            target = np.floor(z) + f32(0.5) + off
+        pos[:, 2] += ((target - z) / f32(p.rdh)).astype(np.float32)
+    ri, rf = O.index_probe(tb, pos)
+    z = ((pos[:, 2] - rf[:, 0]) - f32(p.hmin)) * f32(p.rdh)
+    fr = np.abs(z - np.floor(z) - f32(0.5))
+    keep = fr != 0  # exact ties round differently on the two sides (half away from zero / to even)
+    assert keep.mean() > 0.85 and (fr[keep] < 2e-3).mean() > 0.5
+    torch = _torch()
+    dpos = torch.from_numpy(pos).cuda()
+    oi = torch.zeros((len(pos), 8), dtype=torch.int32, device="cuda")
+    of = torch.zeros((len(pos), 2), dtype=torch.float32, device="cuda")
+    c.index_probe_device(dpos.data_ptr(), len(pos), oi.data_ptr(), of.data_ptr())
+    torch.cuda.synchronize()
+    gi = oi.cpu().numpy()
+    bad = np.argwhere((gi[:, 0] != ri[:, 0]) & keep)
+    assert len(bad) == 0, (bad[:5], z[bad[:5, 0]])
+    c.close()
+
+
 def _generate(c, bunches, num):
     torch = _torch()
     db = _dev(bunches)
