@@ -159,6 +159,72 @@ def plain_kernel_sample(photons, events, local):
     return x
 
 
+def gradient_sample(local, events=64, photons=10_000_000, steps=3, plain_kernel=True):
+    """Ice gradient over the 342 per-layer coefficients: 64 flasher events of 1e7 photons
+    (12-fold LEDs at 30 degrees on distinct random DOMs), Poisson log-likelihood of the
+    per-(event, DOM) charges against charges drawn from a hidden ice (each layer's be and ba
+    scaled by U(0.9, 1.1)).  One evaluation = recording forward + replay, through
+    PPC.gradient with host buffers.  The comparison is a central finite-difference gradient,
+    2 x 342 forward runs, with the reference's CUDA kernel (one eout() per event)."""
+    from ppc_b200 import workloads as W
+    from ppc_b200.api import PPC
+
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    c = PPC()
+    c.initialize(1.0, ice)
+    c.set_seed(4242)
+    c.choose(local)
+    c.ini()
+    oms = c.tables()["oms"]
+    rng = np.random.default_rng(64)
+    doms = rng.choice(len(oms), events, replace=False)
+    b = np.concatenate([W.flasher(int(k), oms["r"][k], photons, q=i) for i, k in enumerate(doms)])
+    be0, ba0 = c.get_ice()
+    n = len(be0)
+    c.set_ice((be0 * rng.uniform(0.9, 1.1, n)).astype(np.float32), (ba0 * rng.uniform(0.9, 1.1, n)).astype(np.float32))
+    gs = c.info()["gsize"]
+    mu = c.gradient(b, weights=np.zeros(events * gs, np.float32), events=events)["counts"]
+    obs = rng.poisson(mu).astype(np.float32)
+    c.set_ice(be0, ba0)
+    c.gradient(b, observed=obs, events=events)  # warm-up
+    wall, fwd, bwd, hits = [], [], [], 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        r = c.gradient(b, observed=obs, events=events)
+        wall.append(time.perf_counter() - t0)
+        fwd.append(r["info"]["forward_ms"])
+        bwd.append(r["info"]["backward_ms"])
+        hits = r["info"]["hits"]
+        unmatched = r["info"]["unmatched"]
+    c.close()
+    out = {
+        "evals_per_s": steps / sum(wall), "unit": "gradient evals/s (342 parameters)",
+        "workload": f"{events} flasher events x {photons:.0e} photons, 12-fold LEDs at 30 deg, per-(event, DOM) "
+                    "Poisson log-likelihood, hidden ice +-10% per layer",
+        "forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
+        "backward_over_forward": statistics.median(bwd) / statistics.median(fwd),
+        "wall_s": statistics.median(wall), "hits": hits, "unmatched_replays": unmatched,
+    }
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
+    if plain_kernel and os.path.exists(exe):
+        path = os.path.join(tempfile.mkdtemp(), "flashers.txt")
+        with open(path, "w") as f:
+            for k in doms:
+                f.write(f"F {int(k) // 60 + 1} {int(k) % 60 + 1} {photons}\n")
+        env = dict(os.environ, PPCTABLESDIR=ice, CUDA_VISIBLE_DEVICES=str(local), FLDR="3960", ELEV="30")
+        p = subprocess.run([exe, "file:" + path, "0", "0", "1"], env=env, capture_output=True, text=True, timeout=900)
+        lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+        if p.returncode == 0 and lines:
+            x = json.loads(lines[-1])
+            fd_s = 2 * 2 * n * x["wall_s"]
+            out["fd_plain_kernel"] = {"forward_wall_s": x["wall_s"], "forward_device_ms": x["device_ms"],
+                                      "fd_gradient_s": fd_s, "evals_per_s": 1.0 / fd_s,
+                                      "kind": "central differences, 2 x 342 forward runs of the reference CUDA "
+                                              "kernel (gpu/pro.cu, sm_100a), one eout() per event"}
+            out["speedup_vs_fd_plain_kernel"] = out["evals_per_s"] * fd_s
+    return out
+
+
 def run_batched(args, local):
     """4096 events (log-uniform 1e3-1e7 photons; half flashers on random DOMs, 12-fold at
     30 degrees, half cascades) in one graph-replayed launch, against the reference's CUDA
@@ -399,6 +465,12 @@ def run_ours(args, rank, world, local):
                                     "photons": pk["photons"],
                                     "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, gpu/Makefile flags",
                                     "speedup": value / pk["value"]}
+    if not args.no_gradient:
+        if args.no_plain_kernel:
+            del d_hits, flush
+            torch.cuda.empty_cache()
+            c.close()
+        line["gradient"] = gradient_sample(local, plain_kernel=not args.no_plain_kernel)
     if not args.no_cpu_baseline:
         r = cpu_reference_sample(args.ref_photons, os.cpu_count() or 1)
         if r:
@@ -422,6 +494,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the ice-gradient evaluation")
     ap.add_argument("--config", default="cascade", choices=["cascade", "batched"],
                     help="cascade: the headline workload; batched: 4096 events in one launch")
     ap.add_argument("--events", type=int, default=4096)

@@ -79,10 +79,11 @@ int ppcb_destroy(ppcb_ctx* c);                                       /* stop(), 
 int ppcb_initialize(ppcb_ctx* c, const char* tables_dir, float enh); /* initialize(), gpu/ppc.cu:36; dir NULL: PPCTABLESDIR */
 int ppcb_choose(ppcb_ctx* c, int device);                            /* choose(), gpu/ppc.cu:490-508 */
 int ppcb_set_seed(ppcb_ctx* c, uint32_t seed);                       /* fixed seed instead of the clock (gpu/ini.cxx:792-795, DTMN) */
-/* deterministic: 0 photons taken dynamically (fastest); 1 photon i on thread i mod T, in the
- * reference's order; 2 as 1 and each photon draws from its own stream keyed by (seed, i), so
- * two runs that differ only in the ice share every photon's random numbers (common random
- * numbers for finite differences and fits).  No counterpart in the reference. */
+/* deterministic: 0 photons taken dynamically, one random stream per thread (fastest);
+ * 1 photon i on thread i mod T with the thread streams, the reference's order; 2 photons taken
+ * dynamically, each drawing from its own stream keyed by (seed, i), so two runs that differ
+ * only in the ice share every photon's random numbers (common random numbers for finite
+ * differences and fits).  Mode 2 has no counterpart in the reference. */
 int ppcb_set_options(ppcb_ctx* c, int deterministic, uint32_t max_steps, int blocks_per_sm);
 int ppcb_ini(ppcb_ctx* c);                                           /* ini(), gpu/ppc.cu:330-361 */
 int ppcb_fin(ppcb_ctx* c);                                           /* fin(), gpu/ppc.cu:398-402 */
@@ -194,7 +195,11 @@ int ppcb_batch_autotune(ppcb_batch* b, const ppcb_bunch* bunches, int32_t nb, ui
  * photons to form d/d be_j and d/d ba_j (FP64, file order) of
  *   LL = sum_d (k_d log mu_d - mu_d)   with `observed` k_d (DOMs with mu_d = 0 left out), or
  *   sum_d w_d mu_d                     with `weights` w_d when observed is NULL,
- * where mu_d = scale x (simulated hits on DOM d).  Absorption terms are pathwise
+ * where mu_d = scale x (simulated hits in charge bin d).  The charge bins are the DOMs
+ * (events = 0; observed/weights/counts hold gsize values) or, with events > 0, the
+ * (event, DOM) pairs, the event being the hit's segment id (the bunch's q): bin =
+ * event x gsize + DOM, events x gsize values, hits of segments >= events left out.
+ * Absorption terms are pathwise
  * (-nr L_j dabs/dba), scattering terms score-function ((n_j/sca_j - L_j) dsca/dbe). */
 typedef struct ppcb_grad_info {
   double ll;
@@ -203,8 +208,9 @@ typedef struct ppcb_grad_info {
 } ppcb_grad_info;
 int ppcb_set_ice(ppcb_ctx* c, const float* be, const float* ba);
 int ppcb_get_ice(ppcb_ctx* c, float* be, float* ba, int32_t* size);
-int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, const float* observed, const float* weights,
-                  double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba, ppcb_grad_info* info);
+int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t events, const float* observed,
+                  const float* weights, double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba,
+                  ppcb_grad_info* info);
 
 /* ---- propagation that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device memory while

@@ -125,7 +125,7 @@ def lib():
         "ppcb_batch_autotune": (i32, [vp, vp, i32, u32, u64, P(TuneInfo)]),
         "ppcb_set_ice": (i32, [vp, vp, vp]),
         "ppcb_get_ice": (i32, [vp, vp, vp, P(i32)]),
-        "ppcb_gradient": (i32, [vp, vp, i32, vp, vp, f64, u64, vp, vp, vp, P(GradInfo)]),
+        "ppcb_gradient": (i32, [vp, vp, i32, u32, vp, vp, f64, u64, vp, vp, vp, P(GradInfo)]),
         "ppcb_fp32_peak": (i32, [i32, i32, P(f64), P(f64)]),
     }
     for name, (res, args) in sig.items():

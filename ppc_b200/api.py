@@ -40,8 +40,8 @@ class PPC:
         check(lib().ppcb_set_seed(self._c, int(seed) & 0xFFFFFFFF))
 
     def set_options(self, deterministic=False, max_steps=1_000_000, blocks_per_sm=0, photon_streams=False):
-        """deterministic: photon i on thread i mod T (the reference's order).  photon_streams
-        (implies deterministic): each photon draws from its own stream keyed by (seed, i), so
+        """deterministic: photon i on thread i mod T (the reference's order).  photon_streams:
+        each photon draws from its own stream keyed by (seed, i), whatever thread runs it, so
         runs that differ only in the ice share every photon's random numbers."""
         mode = 2 if photon_streams else int(bool(deterministic))
         check(lib().ppcb_set_options(self._c, mode, int(max_steps), int(blocks_per_sm)))
@@ -281,22 +281,30 @@ def _ice_methods():
         check(lib().ppcb_get_ice(self._c, _p(be), _p(ba), C.byref(n)))
         return be, ba
 
-    def gradient(self, bunches, observed=None, weights=None, scale=1.0, hit_cap=None):
-        """LL (or sum_d w_d mu_d) and its gradient in (be, ba), file order (ppcb_gradient)."""
+    def gradient(self, bunches, observed=None, weights=None, scale=1.0, hit_cap=None, events=0):
+        """LL (or sum_d w_d mu_d) and its gradient in (be, ba), file order (ppcb_gradient).
+        Charge bins: per DOM (events=0), or per (event, DOM) with the event = the bunch's q
+        (observed / weights / counts then have shape (events, gsize))."""
         from ._lib import GradInfo
         bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
         info_ = self.info()
         gsize, size = info_["gsize"], info_["size"]
         if hit_cap is None:
             hit_cap = int(bunches["num"].sum() * 0.02) + (1 << 16)
-        obs = None if observed is None else np.ascontiguousarray(observed, np.float32)
-        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
-        counts = np.zeros(gsize, np.uint32)
+        nbins = gsize * (events if events else 1)
+        obs = None if observed is None else np.ascontiguousarray(observed, np.float32).reshape(-1)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32).reshape(-1)
+        for name, x in (("observed", obs), ("weights", w)):
+            if x is not None and x.size != nbins:
+                raise ValueError(f"{name}: {x.size} values for {nbins} charge bins")
+        counts = np.zeros(nbins, np.uint32)
         g_be = np.zeros(size, np.float64)
         g_ba = np.zeros(size, np.float64)
         gi = GradInfo()
-        check(lib().ppcb_gradient(self._c, _p(bunches), len(bunches), _p(obs), _p(w), float(scale), int(hit_cap),
-                                  _p(counts), _p(g_be), _p(g_ba), C.byref(gi)))
+        check(lib().ppcb_gradient(self._c, _p(bunches), len(bunches), int(events), _p(obs), _p(w), float(scale),
+                                  int(hit_cap), _p(counts), _p(g_be), _p(g_ba), C.byref(gi)))
+        if events:
+            counts = counts.reshape(events, gsize)
         return {"ll": gi.ll, "counts": counts, "g_be": g_be, "g_ba": g_ba,
                 "info": {k: getattr(gi, k) for k, _ in GradInfo._fields_}}
 

@@ -124,11 +124,12 @@ int ppcb_get_ice(ppcb_ctx* c, float* be, float* ba, int32_t* size) {
   });
 }
 
-int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, const float* observed, const float* weights,
-                  double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba, ppcb_grad_info* info) {
+int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t events, const float* observed,
+                  const float* weights, double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba,
+                  ppcb_grad_info* info) {
   if (!c || !bunches) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
   return bguard([&] {
-    ppcb::Engine::Grad r = c->s.eng.gradient(bunches, nb, observed, weights, scale, hit_cap);
+    ppcb::Engine::Grad r = c->s.eng.gradient(bunches, nb, events, observed, weights, scale, hit_cap);
     const int size = c->s.eng.cfg.p.size;
     if (counts) memcpy(counts, r.counts.data(), r.counts.size() * sizeof(uint32_t));
     if (g_be) memcpy(g_be, r.g_be.data(), size * sizeof(double));

@@ -103,17 +103,18 @@ class Engine {
 
   struct Grad {
     double ll = 0;                   // Poisson log-likelihood sum_d (k_d log mu_d - mu_d) over DOMs with mu_d > 0
-    std::vector<uint32_t> counts;    // simulated hits per DOM
+    std::vector<uint32_t> counts;    // simulated hits per charge bin
     std::vector<double> g_be, g_ba;  // d/d be_j, d/d ba_j in file order (icemodel.dat rows)
     uint64_t photons = 0, hits = 0, replayed = 0, unmatched = 0, steps = 0;
     float forward_ms = 0, backward_ms = 0;
   };
-  // Gradient of sum_d w_d mu_d, mu_d = scale x (simulated hits on DOM d), with respect to the
-  // 2 x size ice coefficients.  With `observed` (per DOM) w_d = dLL/dmu_d of the Poisson
-  // log-likelihood; otherwise `weights` (per DOM) are used as given.  One recording
+  // Gradient of sum_d w_d mu_d, mu_d = scale x (simulated hits in charge bin d), with respect
+  // to the 2 x size ice coefficients.  The bins are the DOMs (events = 0) or the (event, DOM)
+  // pairs, event = hit segment id < events.  With `observed` (per bin) w_d = dLL/dmu_d of the
+  // Poisson log-likelihood; otherwise `weights` (per bin) are used as given.  One recording
   // forward launch over the bunches (device 0) and one replay of the recorded hits.
-  Grad gradient(const ppcb_bunch* b, int nb, const float* observed, const float* weights, double scale,
-                uint64_t hit_cap);
+  Grad gradient(const ppcb_bunch* b, int nb, uint32_t events, const float* observed, const float* weights,
+                double scale, uint64_t hit_cap);
   double total_device_ms() const;
   KArgs args_for(int d) const;
 

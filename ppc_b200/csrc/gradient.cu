@@ -27,14 +27,15 @@ struct DBuf {
 };
 }  // namespace
 
-Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, const float* observed, const float* weights, double scale,
-                              uint64_t hit_cap) {
+Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, const float* observed,
+                              const float* weights, double scale, uint64_t hit_cap) {
   if (!inited_) throw Error("ini() must come before the gradient", 6);
   if (nb <= 0) throw Error("no bunches", 7);
   if (!observed && !weights) throw Error("gradient: observed counts or DOM weights required", 7);
   DeviceCtx& g = devs[0];
   check(cudaSetDevice(g.dev), "cudaSetDevice");
   const int gsize = cfg.p.gsize, size = cfg.p.size;
+  const size_t nbins = (size_t)gsize * (events ? events : 1);  // charge bins: DOM, or (event, DOM)
   std::vector<uint64_t> bs(nb + 1, 0);
   for (int k = 0; k < nb; k++) bs[k + 1] = bs[k] + b[k].num;
   DBuf<ppcb_bunch> db(nb);
@@ -42,8 +43,8 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, const float* observed
   DBuf<ppcb_hit> dh(hit_cap);
   DBuf<unsigned char> dprov(hit_cap * kProvBytes);
   DBuf<ppcb_ctrl> dctrl(1);
-  DBuf<unsigned int> dcnt(gsize);
-  DBuf<float> dw(gsize);
+  DBuf<unsigned int> dcnt(nbins);
+  DBuf<float> dw(nbins);
   DBuf<float2> dwg(PPCB_WNUM);
   DBuf<double> dgo(2 * PPCB_MAXLYS);
   DBuf<unsigned int> dstat(2);
@@ -52,7 +53,7 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, const float* observed
   check(cudaMemcpyAsync(dbs.p, bs.data(), (nb + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "H2D offsets");
   check(cudaMemcpyAsync(dwg.p, cfg.wgrad.data(), PPCB_WNUM * sizeof(float2), cudaMemcpyHostToDevice, st), "H2D");
   check(cudaMemsetAsync(dctrl.p, 0, sizeof(ppcb_ctrl), st), "memset");
-  check(cudaMemsetAsync(dcnt.p, 0, gsize * sizeof(unsigned int), st), "memset");
+  check(cudaMemsetAsync(dcnt.p, 0, nbins * sizeof(unsigned int), st), "memset");
   check(cudaMemsetAsync(dgo.p, 0, 2 * PPCB_MAXLYS * sizeof(double), st), "memset");
   check(cudaMemsetAsync(dstat.p, 0, 2 * sizeof(unsigned int), st), "memset");
   cudaEvent_t e0, e1, e2;
@@ -72,15 +73,15 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, const float* observed
   check(cudaStreamSynchronize(st), "recording pass");
   const uint64_t nh = std::min<uint64_t>(c.hidx, hit_cap);
   if (c.hidx > hit_cap) throw Error("gradient: hit capacity too small (" + std::to_string(c.hidx) + " hits)", 7);
-  check(launch_dom_hist(dh.p, nh, dcnt.p, st), "histogram");
+  check(launch_dom_hist(dh.p, nh, dcnt.p, events, gsize, st), "histogram");
   Grad out;
-  out.counts.resize(gsize);
-  check(cudaMemcpyAsync(out.counts.data(), dcnt.p, gsize * sizeof(unsigned int), cudaMemcpyDeviceToHost, st), "D2H");
+  out.counts.resize(nbins);
+  check(cudaMemcpyAsync(out.counts.data(), dcnt.p, nbins * sizeof(unsigned int), cudaMemcpyDeviceToHost, st), "D2H");
   check(cudaStreamSynchronize(st), "histogram");
-  // per-DOM weights: dLL/dmu_d = k_d/mu_d - 1 (times d mu_d / d count = scale)
-  std::vector<float> w(gsize, 0.f);
+  // per-bin weights: dLL/dmu_d = k_d/mu_d - 1 (times d mu_d / d count = scale)
+  std::vector<float> w(nbins, 0.f);
   double ll = 0;
-  for (int d = 0; d < gsize; d++) {
+  for (size_t d = 0; d < nbins; d++) {
     const double mu = scale * out.counts[d];
     if (observed) {
       if (mu > 0) {
@@ -90,11 +91,11 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, const float* observed
     } else w[d] = (float)(scale * weights[d]);
   }
   out.ll = ll;
-  check(cudaMemcpyAsync(dw.p, w.data(), gsize * sizeof(float), cudaMemcpyHostToDevice, st), "H2D weights");
+  check(cudaMemcpyAsync(dw.p, w.data(), nbins * sizeof(float), cudaMemcpyHostToDevice, st), "H2D weights");
   // replay of the detected photons
   KArgs r = args_for(0);
   r.ctrl = dctrl.p;
-  check(launch_adjoint(r, dh.p, dprov.p, nh, dw.p, dwg.p, dgo.p, dstat.p, g.prop.multiProcessorCount * 4, st),
+  check(launch_adjoint(r, dh.p, dprov.p, nh, events, dw.p, dwg.p, dgo.p, dstat.p, g.prop.multiProcessorCount * 4, st),
         "replay launch");
   check(cudaEventRecord(e2, st), "event");
   std::vector<double> go(2 * PPCB_MAXLYS);

@@ -466,7 +466,7 @@ struct AdjHook {
   double* g_be;
   double* g_ba;
   Prov* prov_out;      // recording: provenance array, indexed like the hits
-  Prov start;          // recording: this thread's current photon
+  Prov* start;         // recording: this thread's current photon (a shared-memory slot)
   __device__ __forceinline__ bool active() const { return replay && !done; }
   // path length `del` from layer coordinate z (layer I), direction sign/anz, layer step edh.
   // The hook's arithmetic is in explicitly rounded intrinsics, which the compiler neither
@@ -503,7 +503,7 @@ struct AdjHook {
     }
     const unsigned long long slot = emit_hit(a, h);
     if (prov_out && slot < a.hcap) {
-      Prov p = start;
+      Prov p = *start;
       p.s.w = (unsigned)ph.nhit;
       prov_out[slot] = p;
     }
@@ -841,28 +841,39 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
 // long and branchy (source type, gamma profile, Cherenkov cone); done by the one or two
 // lanes whose photon just died it runs at 1/32 SIMT efficiency.  Instead the whole warp
 // samples up to 32 photons at once into the pool, and lanes whose photon died take one
-// from the pool (three 16-byte shared-memory loads).
+// from the pool (three 16-byte shared-memory loads).  With per-photon streams the pool
+// also carries each photon's stream state.
+template <bool STREAMS>
 struct PhotonPool {
   float4 r[32];
   float4 n[32];
-  int4 m[32];  // wavelength bin, segment, flasher DOM, veto code
-  int count;
+  int4 m[32];                   // wavelength bin, segment, flasher DOM, veto code
+  uint4 st[STREAMS ? 32 : 1];   // per-photon streams: state x, y and multiplier index
 };
 
-template <int BLOCK, int MINB, bool REC>
+// Random streams.  Thread streams (STREAMS = false, the reference's scheme): each thread
+// owns one MWC stream that runs on from photon to photon and from launch to launch.
+// Per-photon streams (STREAMS = true): photon i starts from photon_stream(seed, i) with
+// multiplier rm[i mod min(T, 1024)], and its state travels with it through the pool, so
+// its random numbers do not depend on which lane samples or propagates it or on what ran
+// before -- two launches that differ only in the ice see the same numbers per photon.
+template <int BLOCK, int MINB, bool REC, bool STREAMS>
 __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant__ KArgs a) {
   __shared__ SmemTables S;
-  __shared__ PhotonPool pools[BLOCK / 32];
+  __shared__ PhotonPool<STREAMS> pools[BLOCK / 32];
+  extern __shared__ Prov snaps[];  // recording: BLOCK slots, each thread's current photon at pick-up
   load_tables(a, S);
   // launch sizes: from the parameters, or from device memory for replayed graphs
   const uint64_t num = a.dyn ? a.dyn[0] : a.num;
   const int nb = a.dyn ? (int)a.dyn[1] : a.nb;
   const uint32_t T = gridDim.x * blockDim.x;
   const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nmul = T < 1024u ? T : 1024u;  // multipliers used by per-photon streams
   const unsigned int lane = threadIdx.x & 31;
   const unsigned int FULL = 0xffffffffu;
-  PhotonPool& P = pools[threadIdx.x >> 5];
+  PhotonPool<STREAMS>& P = pools[threadIdx.x >> 5];
   Rng s;
+  uint32_t mi = gt;  // multiplier index of the stream in s
   {
     uint64_t st = a.rs[gt];
     s.x = (uint32_t)st; s.y = (uint32_t)(st >> 32); s.a = a.rm[gt];
@@ -881,18 +892,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
     hk.replay = false;
     hk.done = false;
     hk.prov_out = static_cast<Prov*>(a.prov);
+    hk.start = &snaps[threadIdx.x];
   }
   // every lane of the warp stays in this loop until the warp is done, so the warp-wide
   // operations below always see all 32 lanes
   while (true) {
     const unsigned int dead = __ballot_sync(FULL, !alive);
     if (dead && !(exhausted && have == 0)) {
-      // --- sample: each generating lane produces one photon from its own stream
+      // --- sample: each generating lane produces one photon
       bool gen = false;
       uint64_t gidx = 0;
       unsigned long long base = 0;
       int ngen = 0;
-      if (a.deterministic) {  // photon i on thread i mod T, as the oracle sequences it
+      if (a.deterministic == 1) {  // photon i on thread i mod T, as the oracle sequences it
         gen = !alive && sidx < num;
         gidx = sidx;
         if (!alive) sidx += T;
@@ -905,15 +917,29 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
         if (base + ngen >= num) exhausted = true;
       }
       Photon g;
+      uint4 gst = make_uint4(0, 0, 0, 0);
       if (gen) {
-        if (a.deterministic == 2) photon_stream(s, gidx, a.seed);
         hint = find_bunch(a, nb, gidx, hint);
-        const Sampled smp = sample_photon(a, hint, s.x, s.y, s.a);
-        g = smp.ph;
-        s.x = smp.x; s.y = smp.y;
+        if constexpr (STREAMS) {  // the photon's own stream; the lane's s is left alone
+          Rng sg;
+          const uint32_t m = (uint32_t)(gidx % nmul);
+          sg.a = a.rm[m];
+          photon_stream(sg, gidx, a.seed);
+          const Sampled smp = sample_photon(a, hint, sg.x, sg.y, sg.a);
+          g = smp.ph;
+          gst = make_uint4(smp.x, smp.y, m, 0);
+        } else {
+          const Sampled smp = sample_photon(a, hint, s.x, s.y, s.a);
+          g = smp.ph;
+          s.x = smp.x; s.y = smp.y;
+        }
       }
-      if (a.deterministic) {
-        if (gen) { ph = g; alive = true; }
+      if (a.deterministic == 1) {
+        if (gen) {
+          ph = g;
+          alive = true;
+          if constexpr (STREAMS) { s.x = gst.x; s.y = gst.y; mi = gst.z; s.a = a.rm[mi]; }
+        }
         exhausted = __all_sync(FULL, sidx >= num);
       } else {
         if (gen) {
@@ -921,6 +947,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
           P.r[slot] = g.r;
           P.n[slot] = g.n;
           P.m[slot] = make_int4(g.wl, (int)g.niw, g.om0, g.ofla);
+          if constexpr (STREAMS) P.st[slot] = gst;
         }
         have += __popc(__ballot_sync(FULL, gen));
         __syncwarp();
@@ -932,6 +959,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
           ph.n = P.n[slot];
           const int4 m = P.m[slot];
           ph.wl = m.x; ph.niw = (uint32_t)m.y; ph.om0 = m.z; ph.ofla = m.w;
+          if constexpr (STREAMS) {
+            const uint4 t = P.st[slot];
+            s.x = t.x; s.y = t.y; mi = t.z; s.a = a.rm[mi];
+          }
           alive = true;
         }
         have -= min(have, __popc(dead));
@@ -940,10 +971,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       if (alive && (dead >> lane & 1u)) {  // a fresh photon: absorption depth, gpu/pro.cu:496-497
         ph.nhit = 0;
         if constexpr (REC) {
-          hk.start.r = ph.r;
-          hk.start.n = ph.n;
-          hk.start.m = make_int4(ph.wl, (int)ph.niw, ph.om0, ph.ofla);
-          hk.start.s = make_uint4(s.x, s.y, gt, 0);
+          hk.start->r = ph.r;
+          hk.start->n = ph.n;
+          hk.start->m = make_int4(ph.wl, (int)ph.niw, ph.om0, ph.ofla);
+          hk.start->s = make_uint4(s.x, s.y, mi, 0);
         }
         ph.TOT = -logf(xrnd(s));
         ph.SCA = 0;
@@ -964,9 +995,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       if (ph.TOT == 0) alive = false;
     }
   }
-  a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
+  if constexpr (!STREAMS) a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
   atomicAdd(&a.ctrl->steps, nsteps);
   if (capped) atomicAdd(&a.ctrl->capped, capped);
+}
+
+// Charge bin of a hit: its DOM, or with `events` > 0 (event, DOM) with the event taken
+// from the hit's segment id; -1 for a segment id outside [0, events).
+__device__ __forceinline__ long long charge_bin(const ppcb_hit& h, uint32_t events, int gsize) {
+  if (!events) return h.i;
+  return h.n < events ? (long long)h.n * gsize + h.i : -1;
 }
 
 // Gradient replay: one thread per recorded hit.  The photon is restarted from its
@@ -976,7 +1014,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
 // recorded hit is reached again.  A replay that does not end on the recorded hit (same
 // DOM, same time bits) is counted in stats[1].
 __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a, const ppcb_hit* __restrict__ hits,
-                                                 const Prov* __restrict__ prov, uint64_t nh,
+                                                 const Prov* __restrict__ prov, uint64_t nh, uint32_t events,
                                                  const float* __restrict__ wdom, const float2* __restrict__ wgrad,
                                                  double* g_out, unsigned int* stats) {
   __shared__ SmemTables S;
@@ -986,7 +1024,8 @@ __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a
   unsigned int nan_steps = 0, replayed = 0, unmatched = 0;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x) {
     const ppcb_hit h = hits[k];
-    const float w = wdom[h.i];
+    const long long bin = charge_bin(h, events, a.p.gsize);
+    const float w = bin >= 0 ? wdom[bin] : 0.f;
     if (w == 0) continue;
     const Prov P = prov[k];
     Rng s;
@@ -1013,6 +1052,7 @@ __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a
     hk.g_be = gbe;
     hk.g_ba = gba;
     hk.prov_out = nullptr;
+    hk.start = nullptr;
     while (!hk.done && ph.TOT != 0 && ph.steps < a.max_steps) {
       step(a, S, ph, s, nan_steps, hk);
       ph.steps++;
@@ -1029,21 +1069,26 @@ __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a
   if (unmatched) atomicAdd(&stats[1], unmatched);
 }
 
-__global__ void k_dom_hist(const ppcb_hit* __restrict__ hits, uint64_t nh, unsigned int* counts) {
-  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x)
-    atomicAdd(&counts[hits[k].i], 1u);
+__global__ void k_dom_hist(const ppcb_hit* __restrict__ hits, uint64_t nh, unsigned int* counts, uint32_t events,
+                           int gsize) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x) {
+    const long long b = charge_bin(hits[k], events, gsize);
+    if (b >= 0) atomicAdd(&counts[b], 1u);
+  }
 }
 
-cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, const float* wdom,
-                           const float2* wgrad, double* g_out, unsigned int* stats, int blocks, cudaStream_t st) {
+cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, uint32_t events,
+                           const float* wdom, const float2* wgrad, double* g_out, unsigned int* stats, int blocks,
+                           cudaStream_t st) {
   if (nh == 0) return cudaSuccess;
-  k_adjoint<<<blocks, 256, 0, st>>>(a, hits, static_cast<const Prov*>(prov), nh, wdom, wgrad, g_out, stats);
+  k_adjoint<<<blocks, 256, 0, st>>>(a, hits, static_cast<const Prov*>(prov), nh, events, wdom, wgrad, g_out, stats);
   return cudaGetLastError();
 }
 
-cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, cudaStream_t st) {
+cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, uint32_t events, int gsize,
+                            cudaStream_t st) {
   if (nh == 0) return cudaSuccess;
-  k_dom_hist<<<592, 256, 0, st>>>(hits, nh, counts);
+  k_dom_hist<<<592, 256, 0, st>>>(hits, nh, counts, events, gsize);
   return cudaGetLastError();
 }
 
@@ -1094,15 +1139,30 @@ __global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos
 }
 
 // Two compiled shapes: 256 threads x 3 blocks per SM and 128 x 6 (the same 768 threads
-// per SM at <= 80 registers); the autotuner picks one.
-cudaError_t launch_propagate(const KArgs& a, LaunchShape sh, cudaStream_t st) {
-  if (a.prov) {  // the gradient's recording pass
+// per SM at <= 80 registers); the autotuner picks one.  Per-photon streams run with
+// deterministic = 2, and in the gradient's recording pass unless the photon order is
+// static (deterministic = 1: thread streams, photon i on thread i mod T, nothing interleaves).
+template <bool REC, bool STREAMS>
+static cudaError_t launch_shape(const KArgs& a, LaunchShape sh, cudaStream_t st) {
+  if constexpr (REC) {
+    constexpr size_t dyn = 256 * sizeof(Prov);
+    cudaError_t e = cudaFuncSetAttribute(k_propagate<256, 3, true, STREAMS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
     if (sh.threads != 256) return cudaErrorInvalidConfiguration;
-    k_propagate<256, 3, true><<<sh.blocks, 256, 0, st>>>(a);
-  } else if (sh.threads == 256) k_propagate<256, 3, false><<<sh.blocks, 256, 0, st>>>(a);
-  else if (sh.threads == 128) k_propagate<128, 6, false><<<sh.blocks, 128, 0, st>>>(a);
+    k_propagate<256, 3, true, STREAMS><<<sh.blocks, 256, dyn, st>>>(a);
+  } else if (sh.threads == 256) k_propagate<256, 3, false, STREAMS><<<sh.blocks, 256, 0, st>>>(a);
+  else if (sh.threads == 128) k_propagate<128, 6, false, STREAMS><<<sh.blocks, 128, 0, st>>>(a);
   else return cudaErrorInvalidConfiguration;
   return cudaGetLastError();
+}
+
+cudaError_t launch_propagate(const KArgs& a, LaunchShape sh, cudaStream_t st) {
+  if (a.deterministic < 0 || a.deterministic > 2) return cudaErrorInvalidValue;
+  if (a.prov) {
+    return a.deterministic == 1 ? launch_shape<true, false>(a, sh, st) : launch_shape<true, true>(a, sh, st);
+  }
+  return a.deterministic == 2 ? launch_shape<false, true>(a, sh, st) : launch_shape<false, false>(a, sh, st);
 }
 
 cudaError_t launch_generate(const KArgs& a, LaunchShape, void* pbuf_out, cudaStream_t st) {
@@ -1121,7 +1181,7 @@ cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t
 
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local) {
   cudaFuncAttributes at;
-  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate<256, 3, false>);
+  cudaError_t e = cudaFuncGetAttributes(&at, k_propagate<256, 3, false, false>);
   if (e != cudaSuccess) return e;
   *regs = at.numRegs;
   *max_threads = at.maxThreadsPerBlock;
@@ -1132,8 +1192,8 @@ cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size
 
 int propagate_max_blocks_per_sm(int threads) {
   int nb = 0;
-  cudaError_t e = threads == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<128, 6, false>, 128, 0)
-                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<256, 3, false>, 256, 0);
+  cudaError_t e = threads == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<128, 6, false, false>, 128, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<256, 3, false, false>, 256, 0);
   return e == cudaSuccess ? nb : 0;
 }
 

@@ -35,9 +35,9 @@ struct KArgs {
   uint64_t hcap;
   ppcb_ctrl* ctrl;
   // options
-  int deterministic;         // 1: photon i runs on thread i % threads (static order);
-                             // 2: as 1, and photon i draws from its own stream (seed, i)
-  uint32_t seed;             // stream seed of mode 2
+  int deterministic;         // 0: dynamic photon order; 1: photon i runs on thread i % threads
+                             // (static order); 2: dynamic, photon i draws from its own stream (seed, i)
+  uint32_t seed;             // per-photon stream seed
   uint32_t max_steps;        // 0: unlimited; else photons stopped after this many steps
   int refill_below;          // photon pool: the warp also resamples when fewer than this are left
   // batched launches (optional, all null otherwise)
@@ -60,9 +60,13 @@ cudaError_t launch_propagate(const KArgs& a, LaunchShape s, cudaStream_t st);
 cudaError_t launch_generate(const KArgs& a, LaunchShape s, void* pbuf_out, cudaStream_t st);
 cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t* out_i, float* out_f,
                                cudaStream_t st);
-cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, const float* wdom,
-                           const float2* wgrad, double* g_out, unsigned int* stats, int blocks, cudaStream_t st);
-cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, cudaStream_t st);
+// Charges are binned per DOM, or with events > 0 per (event, DOM), the event being the
+// hit's segment id (bin = event * gsize + DOM; hits of segments >= events are left out).
+cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, uint32_t events,
+                           const float* wdom, const float2* wgrad, double* g_out, unsigned int* stats, int blocks,
+                           cudaStream_t st);
+cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, uint32_t events, int gsize,
+                            cudaStream_t st);
 constexpr size_t kProvBytes = 64;  // provenance record per hit slot of the gradient's recording pass
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local);
 int propagate_max_blocks_per_sm(int threads);

@@ -165,3 +165,21 @@ def test_flasher_setup_matches_reference_semantics(ice_full, monkeypatch):
     out = c.flshift([1, 0, 0], [0.0, 0.0, 1.0])
     assert np.allclose(out, [1.0, 0.0, 0.0], atol=1e-6)
     c.close()
+
+
+def test_gradient_checks_charge_bin_sizes(ice_small):
+    """PPC.gradient rejects observed/weights arrays whose size is not the number of charge
+    bins (gsize, or events x gsize) before anything reaches the device."""
+    from ppc_b200 import types as T
+    c = PPC()
+    c.initialize(1.0, ice_small)
+    gs = c.info()["gsize"]
+    b = T.bunch_led([0, 0, 0, 0], [0, 0, 1], 0, 10, 1, ka=-1, up=0, fldr=-1)
+    with pytest.raises(ValueError):
+        c.gradient(b, weights=np.zeros(gs + 1, np.float32))
+    with pytest.raises(ValueError):
+        c.gradient(b, observed=np.zeros(gs, np.float32), events=3)
+    with pytest.raises(PPCError) as e:  # right sizes, but no ini(): the library refuses
+        c.gradient(b, weights=np.zeros((3, gs), np.float32), events=3)
+    assert e.value.code == 6
+    c.close()

@@ -42,8 +42,12 @@ def _total_hits(c, b, be, ba, be0, ba0):
         c.set_ice(be0, ba0)
 
 
-def test_replay_retraces_the_recorded_photons(ice_full):
-    c = _ctx(ice_full, deterministic=True)
+@pytest.mark.parametrize("opts", [{"deterministic": True}, {"deterministic": False}, {"photon_streams": True}],
+                         ids=["static", "dynamic", "photon_streams"])
+def test_replay_retraces_the_recorded_photons(ice_full, opts):
+    """Static order replays thread streams; the dynamic photon pool records per-photon
+    streams (a lane's thread stream would interleave with the sampling it does for others)."""
+    c = _ctx(ice_full, **opts)
     b = _bunches(c, 5_000_000)
     r = c.gradient(b, weights=np.ones(c.info()["gsize"], np.float32))
     info = r["info"]
@@ -144,4 +148,24 @@ def test_gradient_costs_at_most_three_forward_passes(ice_full):
     i = r["info"]
     print("forward ms", i["forward_ms"], "backward ms", i["backward_ms"])
     assert i["forward_ms"] + i["backward_ms"] <= 3 * i["forward_ms"], i
+    c.close()
+
+
+def test_per_event_charge_bins(ice_full):
+    """events > 0: charges binned per (event, DOM) with the event = the bunch's q; their sum
+    over events is the per-DOM histogram, and event-independent weights give the per-DOM
+    gradient (per-photon streams make the two runs identical)."""
+    c = _ctx(ice_full)
+    b = _bunches(c, 5_000_000)
+    gs = c.info()["gsize"]
+    v = np.random.default_rng(5).uniform(-1, 1, gs).astype(np.float32)
+    r0 = c.gradient(b, weights=v)
+    r1 = c.gradient(b, weights=np.tile(v, (len(FLASHERS), 1)), events=len(FLASHERS))
+    assert r1["counts"].shape == (len(FLASHERS), gs)
+    assert np.array_equal(r1["counts"].sum(axis=0), r0["counts"])
+    assert r1["counts"][0].sum() > 0 and r1["counts"][1].sum() > 0
+    assert np.allclose(r1["g_ba"], r0["g_ba"], rtol=1e-6, atol=1e-9 * np.abs(r0["g_ba"]).max())
+    assert np.allclose(r1["g_be"], r0["g_be"], rtol=1e-6, atol=1e-9 * np.abs(r0["g_be"]).max())
+    with pytest.raises(ValueError):
+        c.gradient(b, weights=v, events=len(FLASHERS))
     c.close()
