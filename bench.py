@@ -337,6 +337,7 @@ def run_ours(args, rank, world, local):
     ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
     if not os.path.exists(os.path.join(ice, "cfg.txt")):
         synth.write("full", ice)
+    from ppc_b200.replicas import max_over_ranks
     dist = world > 1
     if dist:
         import torch.distributed as td
@@ -387,11 +388,8 @@ def run_ours(args, rank, world, local):
         hits += ctrl.hidx
     torch.cuda.synchronize()
     clocks = clk.stop() if clk else None
-    total_ms = sum(times)
+    total_ms = max_over_ranks(sum(times))  # the job is as slow as its slowest rank
     if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        total_ms = float(t.item())
         td.barrier()
 
     # end to end through the host API: bunch upload, launch, hit download
@@ -407,11 +405,7 @@ def run_ours(args, rank, world, local):
         if k >= args.warmup:
             e2e_times.append(t1 - t0)
             e2e_hits += len(h)
-    e2e_total = sum(e2e_times) if e2e_times else float("nan")
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(sum(e2e_times) if e2e_times else float("nan"))
 
     if rank != 0:
         return
