@@ -225,6 +225,124 @@ def gradient_sample(local, events=64, photons=10_000_000, steps=3, plain_kernel=
     return out
 
 
+def run_fit(args, local):
+    """Ice fit: 1024 flashers (log-uniform 1e5-1e7 photons, 12-fold LEDs at 30 degrees on
+    distinct random DOMs) and 256 EM cascades (log-uniform 1e6-1e8 photons, vertex in
+    |x|,|y|,|z| <= 500 m, isotropic directions); charges simulated with a hidden ice (be and
+    ba scaled by exp(0.1 x a smooth depth profile)) and other random numbers; L-BFGS over
+    the 342 coefficients on the adjoint gradient with a smoothness penalty.  Compared with an iteration that takes its
+    gradient from central differences of the reference's CUDA kernel (2 x 342 forward runs)."""
+    import torch
+    from ppc_b200 import synth
+    from ppc_b200 import workloads as W
+    from ppc_b200.api import PPC
+    from ppc_b200.fit import fit_ice
+
+    torch.cuda.set_device(local)
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    if not os.path.exists(os.path.join(ice, "cfg.txt")):
+        synth.write("full", ice)
+    rng = np.random.default_rng(55)
+    s = args.fit_scale
+
+    def ctx(seed):
+        c = PPC()
+        c.initialize(1.0, ice)
+        c.set_seed(seed)
+        c.set_options(photon_streams=True)
+        c.choose(local)
+        c.ini()
+        return c
+
+    truth = ctx(901)
+    oms = truth.tables()["oms"]
+    be0, ba0 = truth.get_ice()
+    n = len(be0)
+    nf, nc = 1024, 256
+    doms = rng.choice(len(oms), nf, replace=False)
+    nfl = np.exp(rng.uniform(np.log(1e5), np.log(1e7), nf)) * s
+    ncs = np.exp(rng.uniform(np.log(1e6), np.log(1e8), nc)) * s
+    parts = [W.flasher(int(k), oms["r"][k], int(nfl[i]), q=i) for i, k in enumerate(doms)]
+    cas = []
+    for j in range(nc):
+        v = rng.uniform(-500, 500, 3)
+        ct = rng.uniform(-1, 1)
+        ph = rng.uniform(0, 2 * math.pi)
+        st = math.sqrt(1 - ct * ct)
+        d = [st * math.cos(ph), st * math.sin(ph), ct]
+        parts.append(W.cascade(v, d, int(ncs[j]), q=nf + j))
+        cas.append((v, d, int(ncs[j])))
+    b = np.concatenate(parts)
+    events = nf + nc
+    photons = int(b["num"].sum())
+    hit_cap = int(photons * 0.004) + (1 << 20)
+    def field():  # smooth unit-variance depth profile (Gaussian kernel, 4 layers)
+        x = rng.normal(size=n + 20)
+        k = np.exp(-0.5 * (np.arange(-10, 11) / 4.0) ** 2)
+        f = np.convolve(x, k / k.sum(), mode="same")[10:10 + n]
+        return f / f.std()
+
+    be_t = (be0 * np.exp(0.1 * field())).astype(np.float32)
+    ba_t = (ba0 * np.exp(0.1 * field())).astype(np.float32)
+    truth.set_ice(be_t, ba_t)
+    gs = truth.info()["gsize"]
+    obs = truth.gradient(b, weights=np.zeros(events * gs, np.float32), events=events,
+                         hit_cap=hit_cap)["counts"].astype(np.float32)
+    truth.close()
+    c = ctx(17)
+    g0 = c.gradient(b, observed=obs, events=events, hit_cap=hit_cap)
+    lit_be = np.abs(g0["g_be"] * be0) > 0.05 * np.abs(g0["g_be"] * be0).max()
+    lit_ba = np.abs(g0["g_ba"] * ba0) > 0.05 * np.abs(g0["g_ba"] * ba0).max()
+    clk = Clocks(local)
+    smooth = 3e-3 * float(obs.sum())  # penalty on layer-to-layer differences, scaled with the data
+    r = fit_ice(c, b, obs, events, iters=args.fit_iters, hit_cap=hit_cap, smooth=smooth)
+    clocks = clk.stop()
+    c.close()
+
+    def rms(x, t, m):
+        return float(np.sqrt(np.mean((x[m] / t[m] - 1) ** 2)))
+
+    line = {
+        "metric": "ice-fit seconds per L-BFGS iteration", "value": r["seconds_per_iteration"],
+        "unit": "s/iteration", "n_gpus": 1, "steps": r["iterations"], "warmup": 1,
+        "ms_per_step": 1000 * r["seconds_per_iteration"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 gradient sums)", "data": "synthetic",
+        "config": {"workload": f"{nf} flashers (1e5-1e7 photons) + {nc} cascades (1e6-1e8), full detector, "
+                               "per-(event, DOM) Poisson LL, hidden ice = start x exp(0.1 x smooth unit field) "
+                               "in be and ba, 342 parameters, smoothness penalty 3e-3 x total charge",
+                   "photons_per_evaluation": photons, "photon_scale": s, "observed_charge": float(obs.sum())},
+        "evaluations": r["evaluations"], "ll_first": r["history"][0]["ll"], "ll_final": r["ll"],
+        "forward_ms_median": statistics.median(h["forward_ms"] for h in r["history"]),
+        "backward_ms_median": statistics.median(h["backward_ms"] for h in r["history"]),
+        "recovery": {"lit_layers_be": int(lit_be.sum()), "lit_layers_ba": int(lit_ba.sum()),
+                     "rms_rel_error_be": [rms(be0, be_t, lit_be), rms(r["be"], be_t, lit_be)],
+                     "rms_rel_error_ba": [rms(ba0, ba_t, lit_ba), rms(r["ba"], ba_t, lit_ba)]},
+        "gpu_launches": 3 * r["evaluations"], "clocks": clocks, "accepted_steps": r["accepted"],
+    }
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
+    if not args.no_plain_kernel and os.path.exists(exe):
+        path = os.path.join(tempfile.mkdtemp(), "fit_events.txt")
+        with open(path, "w") as f:
+            for i, k in enumerate(doms):
+                f.write(f"F {int(k) // 60 + 1} {int(k) % 60 + 1} {int(nfl[i])}\n")
+            for v, d, num in cas:
+                E = num * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
+                f.write("C %f %f %f %f %f %f %f %d\n" % (v[0], v[1], v[2], E, d[0], d[1], d[2], num))
+        env = dict(os.environ, PPCTABLESDIR=ice, CUDA_VISIBLE_DEVICES=str(local), FLDR="3960", ELEV="30")
+        p = subprocess.run([exe, "file:" + path, "0", "0", "1"], env=env, capture_output=True, text=True,
+                           timeout=1800)
+        lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+        if p.returncode == 0 and lines:
+            x = json.loads(lines[-1])
+            fd_s = 2 * 2 * n * x["wall_s"]
+            line["fd_plain_kernel"] = {"forward_wall_s": x["wall_s"], "seconds_per_iteration": fd_s,
+                                       "kind": "gradient by central differences, 2 x 342 forward runs of the "
+                                               "reference CUDA kernel, one eout() per event (one forward timed, "
+                                               "x 684)"}
+            line["speedup_vs_fd_plain_kernel"] = fd_s / r["seconds_per_iteration"]
+    print(json.dumps(line))
+
+
 def run_batched(args, local):
     """4096 events (log-uniform 1e3-1e7 photons; half flashers on random DOMs, 12-fold at
     30 degrees, half cascades) in one graph-replayed launch, against the reference's CUDA
@@ -489,8 +607,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")
     ap.add_argument("--no-gradient", action="store_true", help="skip the ice-gradient evaluation")
-    ap.add_argument("--config", default="cascade", choices=["cascade", "batched"],
-                    help="cascade: the headline workload; batched: 4096 events in one launch")
+    ap.add_argument("--config", default="cascade", choices=["cascade", "batched", "fit"],
+                    help="cascade: the headline workload; batched: 4096 events in one launch; "
+                         "fit: L-BFGS ice fit over 1280 events")
+    ap.add_argument("--fit-iters", type=int, default=10)
+    ap.add_argument("--fit-scale", type=float, default=1.0, help="photon counts of the fit workload x this")
     ap.add_argument("--events", type=int, default=4096)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -508,6 +629,8 @@ def main():
             run_reference(args, rank, world)
         elif args.config == "batched":
             run_batched(args, local)
+        elif args.config == "fit":
+            run_fit(args, local)
         else:
             run_ours(args, rank, world, local)
     finally:

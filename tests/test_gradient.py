@@ -169,3 +169,43 @@ def test_per_event_charge_bins(ice_full):
     with pytest.raises(ValueError):
         c.gradient(b, weights=v, events=len(FLASHERS))
     c.close()
+
+
+def _smooth_field(rng, n, corr=4.0):
+    x = rng.normal(size=n + 20)
+    k = np.exp(-0.5 * (np.arange(-10, 11) / corr) ** 2)
+    f = np.convolve(x, k / k.sum(), mode="same")[10:10 + n]
+    return f / f.std()
+
+
+def test_lbfgs_fit_recovers_absorption(ice_full):
+    """L-BFGS on the adjoint gradient, with a smoothness penalty between neighbouring layers,
+    moves the absorption of the illuminated layers towards a hidden ice (ba scaled by
+    exp(0.1 x a smooth unit-variance field in depth)) whose charges were simulated with other
+    random numbers.  Without the penalty the 10 m layers trade off against each other and
+    the fit chases noise."""
+    from ppc_b200.fit import fit_ice
+    rng = np.random.default_rng(21)
+    truth = _ctx(ice_full, seed=99)
+    be0, ba0 = truth.get_ice()
+    oms = truth.tables()["oms"]
+    ne = 64
+    doms = rng.choice(len(oms), ne, replace=False)
+    b = np.concatenate([W.flasher(int(k), oms["r"][k], 3_000_000, q=i) for i, k in enumerate(doms)])
+    ba_true = (ba0 * np.exp(0.1 * _smooth_field(rng, len(ba0)))).astype(np.float32)
+    truth.set_ice(be0, ba_true)
+    gs = truth.info()["gsize"]
+    obs = truth.gradient(b, weights=np.zeros(ne * gs, np.float32), events=ne)["counts"].astype(np.float32)
+    truth.close()
+    c = _ctx(ice_full, seed=7)
+    g0 = c.gradient(b, observed=obs, events=ne)
+    lit = np.abs(g0["g_ba"] * ba0) > 0.1 * np.abs(g0["g_ba"] * ba0).max()
+    r = fit_ice(c, b, obs, ne, iters=15, fit=("ba",), smooth=1e3)
+    err0 = np.sqrt(np.mean((ba0[lit] / ba_true[lit] - 1) ** 2))
+    err1 = np.sqrt(np.mean((r["ba"][lit] / ba_true[lit] - 1) ** 2))
+    lls = [h["ll"] for h in r["history"]]
+    print(f"fit: {lit.sum()} lit layers, rms error {err0:.4f} -> {err1:.4f}, LL {lls[0]:.1f} -> {r['ll']:.1f}, "
+          f"{r['accepted']}/{r['iterations']} steps kept, {r['seconds_per_iteration']:.2f} s/iteration")
+    assert r["ll"] > lls[0]
+    assert err1 < 0.85 * err0
+    c.close()
