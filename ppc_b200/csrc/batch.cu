@@ -223,7 +223,8 @@ TuneResult Batch::autotune(const ppcb_bunch* b, int nb, uint32_t events, uint64_
   const int keep_refill = eng_.refill_below;
   const int Tmax = g.T;
   struct Cand { int threads, per_sm, refill; };
-  const Cand cands[] = {{256, 3, 0}, {128, 6, 0}, {256, 3, 8}, {128, 6, 8}, {256, 2, 0}, {128, 4, 0}, {256, 3, 16}};
+  const Cand cands[] = {{256, 3, 0}, {128, 6, 0}, {768, 1, 0}, {864, 1, 0}, {256, 3, 8},
+                        {768, 1, 8}, {128, 6, 8}, {256, 2, 0}, {256, 3, 16}};
   TuneResult best;
   BatchResult r;
   const bool graph = use_graph;

@@ -80,7 +80,9 @@ void Engine::ini() {
     DeviceCtx& g = devs[k];
     int npho = g.T;
     check(cudaSetDevice(g.dev), "cudaSetDevice");
-    const int kBlock = threads_per_block == 128 ? 128 : 256;
+    int kBlock = threads_per_block;
+    if (const char* t = getenv("PPCB_THREADS_PER_BLOCK")) if (atoi(t) > 0) kBlock = atoi(t);
+    if (kBlock != 128 && kBlock != 256 && kBlock != 768 && kBlock != 864) kBlock = 256;
     int per_sm = blocks_per_sm > 0 ? blocks_per_sm : propagate_max_blocks_per_sm(kBlock);
     if (const char* b = getenv("PPCB_BLOCKS_PER_SM")) if (atoi(b) > 0) per_sm = atoi(b);
     if (per_sm <= 0) per_sm = 1;

@@ -78,7 +78,7 @@ class Engine {
   uint64_t pmax = 0, pmxo = 0;     // photons / bunches per launch
   unsigned int hquo = 1;
   int blocks_per_sm = 0;           // 0: occupancy maximum
-  int threads_per_block = 256;     // 256 or 128 (compiled shapes of the kernel)
+  int threads_per_block = 864;     // 128, 256, 768 or 864 (compiled shapes of the kernel)
   int refill_below = 0;            // photon pool refill threshold (0: refill on demand)
 
   void initialize(const std::string& dir, float enh);

@@ -2,6 +2,7 @@
 // llh/DirectFit fits the ice by repeated forward runs (llh/llh.cxx:1435-1634); here the
 // gradient of the likelihood with respect to all 2 x 171 per-layer coefficients comes from
 // one recording forward pass and a replay of the detected photons (propagate.cu, AdjHook).
+#include <algorithm>
 #include <cmath>
 
 #include "engine.h"
@@ -65,7 +66,9 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, cons
   a.bunches = db.p; a.bstart = dbs.p; a.nb = nb; a.num = bs[nb];
   a.hits = dh.p; a.hcap = hit_cap; a.ctrl = dctrl.p; a.prov = dprov.p;
   check(cudaEventRecord(e0, st), "event");
-  const int rec_blocks = g.shape.threads == 256 ? g.shape.blocks : g.shape.blocks * g.shape.threads / 256;
+  // the recording kernel's shape: 256-thread blocks, all resident at once (a static photon
+  // order must not leave a second wave of blocks), and no more threads than streams
+  const int rec_blocks = std::min(g.prop.multiProcessorCount * propagate_max_blocks_per_sm(256), g.T / 256);
   check(launch_propagate(a, LaunchShape{rec_blocks, 256}, st), "recording launch");
   check(cudaEventRecord(e1, st), "event");
   ppcb_ctrl c;

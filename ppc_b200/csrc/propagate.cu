@@ -21,6 +21,7 @@
 //     same fast-math intrinsics as the reference's GPU build (--use_fast_math).
 #include <cooperative_groups.h>
 
+#include <atomic>
 #include <type_traits>
 
 #include "propagate.cuh"
@@ -857,11 +858,19 @@ struct PhotonPool {
 // multiplier rm[i mod min(T, 1024)], and its state travels with it through the pool, so
 // its random numbers do not depend on which lane samples or propagates it or on what ran
 // before -- two launches that differ only in the ice see the same numbers per photon.
+// Dynamic shared memory of a block: the warps' photon pools, then (recording pass) one
+// provenance slot per thread.
+template <int BLOCK, bool REC, bool STREAMS>
+constexpr size_t dyn_smem() {
+  return (BLOCK / 32) * sizeof(PhotonPool<STREAMS>) + (REC ? BLOCK * sizeof(Prov) : 0);
+}
+
 template <int BLOCK, int MINB, bool REC, bool STREAMS>
 __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant__ KArgs a) {
   __shared__ SmemTables S;
-  __shared__ PhotonPool<STREAMS> pools[BLOCK / 32];
-  extern __shared__ Prov snaps[];  // recording: BLOCK slots, each thread's current photon at pick-up
+  extern __shared__ __align__(16) unsigned char dsm[];
+  PhotonPool<STREAMS>* pools = reinterpret_cast<PhotonPool<STREAMS>*>(dsm);
+  Prov* snaps = reinterpret_cast<Prov*>(dsm + (BLOCK / 32) * sizeof(PhotonPool<STREAMS>));
   load_tables(a, S);
   // launch sizes: from the parameters, or from device memory for replayed graphs
   const uint64_t num = a.dyn ? a.dyn[0] : a.num;
@@ -1138,23 +1147,46 @@ __global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos
   of[2 * k + 1] = dz;
 }
 
-// Two compiled shapes: 256 threads x 3 blocks per SM and 128 x 6 (the same 768 threads
-// per SM at <= 80 registers); the autotuner picks one.  Per-photon streams run with
+// Compiled shapes: 256 threads x 3 blocks per SM, 128 x 6 and 768 x 1 (768 threads per SM
+// at 80 registers), and 864 x 1 (27 warps at 72 registers); the autotuner picks one.  With
+// one block per SM the shared tables are held once instead of three times, which leaves
+// that memory to the L1 cache.  Per-photon streams run with
 // deterministic = 2, and in the gradient's recording pass unless the photon order is
 // static (deterministic = 1: thread streams, photon i on thread i mod T, nothing interleaves).
+// The dynamic shared-memory limit is a per-device function attribute: set it once on each
+// device (before any stream capture that launches the kernel there).
+template <int BLOCK, int MINB, bool REC, bool STREAMS>
+static cudaError_t launch_one(const KArgs& a, int blocks, cudaStream_t st) {
+  constexpr size_t dyn = dyn_smem<BLOCK, REC, STREAMS>();
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(done.load() & bit)) {
+    e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, REC, STREAMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn);
+    if (e != cudaSuccess) return e;
+    done.fetch_or(bit);
+  }
+  k_propagate<BLOCK, MINB, REC, STREAMS><<<blocks, BLOCK, dyn, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <bool REC, bool STREAMS>
 static cudaError_t launch_shape(const KArgs& a, LaunchShape sh, cudaStream_t st) {
   if constexpr (REC) {
-    constexpr size_t dyn = 256 * sizeof(Prov);
-    cudaError_t e = cudaFuncSetAttribute(k_propagate<256, 3, true, STREAMS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-    if (e != cudaSuccess) return e;
     if (sh.threads != 256) return cudaErrorInvalidConfiguration;
-    k_propagate<256, 3, true, STREAMS><<<sh.blocks, 256, dyn, st>>>(a);
-  } else if (sh.threads == 256) k_propagate<256, 3, false, STREAMS><<<sh.blocks, 256, 0, st>>>(a);
-  else if (sh.threads == 128) k_propagate<128, 6, false, STREAMS><<<sh.blocks, 128, 0, st>>>(a);
-  else return cudaErrorInvalidConfiguration;
-  return cudaGetLastError();
+    return launch_one<256, 3, true, STREAMS>(a, sh.blocks, st);
+  } else {
+    switch (sh.threads) {
+      case 256: return launch_one<256, 3, false, STREAMS>(a, sh.blocks, st);
+      case 128: return launch_one<128, 6, false, STREAMS>(a, sh.blocks, st);
+      case 768: return launch_one<768, 1, false, STREAMS>(a, sh.blocks, st);
+      case 864: return launch_one<864, 1, false, STREAMS>(a, sh.blocks, st);
+      default: return cudaErrorInvalidConfiguration;
+    }
+  }
 }
 
 cudaError_t launch_propagate(const KArgs& a, LaunchShape sh, cudaStream_t st) {
@@ -1190,11 +1222,24 @@ cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size
   return cudaSuccess;
 }
 
+template <int BLOCK, int MINB>
+static int max_blocks(int* nb) {
+  constexpr size_t dyn = dyn_smem<BLOCK, false, true>();  // the larger pool (per-photon streams)
+  cudaError_t e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, false, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_propagate<BLOCK, MINB, false, false>, BLOCK, dyn);
+  return e == cudaSuccess ? *nb : 0;
+}
+
 int propagate_max_blocks_per_sm(int threads) {
   int nb = 0;
-  cudaError_t e = threads == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<128, 6, false, false>, 128, 0)
-                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_propagate<256, 3, false, false>, 256, 0);
-  return e == cudaSuccess ? nb : 0;
+  switch (threads) {
+    case 128: return max_blocks<128, 6>(&nb);
+    case 256: return max_blocks<256, 3>(&nb);
+    case 768: return max_blocks<768, 1>(&nb);
+    case 864: return max_blocks<864, 1>(&nb);
+    default: return 0;
+  }
 }
 
 }  // namespace ppcb

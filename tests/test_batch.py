@@ -80,7 +80,7 @@ def test_autotune_picks_a_working_shape(ice_full):
     ev = W.batched_events(c.tables()["oms"], n_events=200, lo=1e3, hi=1e6, seed=1)
     b = Batch(c, max_events=256, max_bunches=256, hit_capacity=1 << 24)
     t = b.autotune(ev, len(ev), sample_photons=5_000_000)
-    assert t["threads"] in (128, 256) and t["photons_per_s"] > 0
+    assert t["threads"] in (128, 256, 768, 864) and t["photons_per_s"] > 0
     info = b.run(ev, len(ev), hits_per_photon=0.05)
     assert info["photons"] == int(ev["num"].sum()) and info["overflowed"] == 0
     b.close()
