@@ -431,13 +431,16 @@ __device__ __forceinline__ unsigned long long emit_hit(const KArgs& a, const ppc
   return base;
 }
 
+// the plain kernel's hit append, out of line (about one step in 2e4 registers a hit)
+__device__ __noinline__ void emit_hit_cold(const KArgs& a, ppcb_hit h) { emit_hit(a, h); }
+
 // ---------------------------------------------------------------- step hooks
 // The plain propagation: hits are appended, nothing else is observed.
 struct NoHook {
   __device__ __forceinline__ bool active() const { return false; }
   __device__ __forceinline__ void segment(int, float, int, float, float, float, float, float, int) {}
   __device__ __forceinline__ void scatter(int, float) {}
-  __device__ __forceinline__ void hit(const KArgs& a, const ppcb_hit& h, Photon&) { emit_hit(a, h); }
+  __device__ __forceinline__ void hit(const KArgs& a, const ppcb_hit& h, Photon&) { emit_hit_cold(a, h); }
 };
 
 // Provenance of a hit, enough to replay its photon: the sampled photon, the stream state
@@ -511,6 +514,84 @@ struct AdjHook {
     ph.nhit++;
   }
 };
+
+// Rare parts of the step, compiled out of line so that the step loop stays small in the
+// instruction cache.
+
+// gpu/pro.cu:655-669: entry and exit of the segment in the hole-ice column of a string
+// (radius hr), given the string's closest-approach terms b, c and np = 1 - nz^2; returns
+// the updated (hi, hf).
+__device__ __noinline__ float2 hole_column(const ppcb_params& e, float b, float c, float np, float sca, float hi,
+                                           float hf) {
+  float DH = b * b - (c - e.hr2) * np;
+  if (DH > 0) {
+    DH = sqrtf(DH);
+    float h1 = b - DH, h2 = b + DH;
+    if (h2 >= 0 && h1 <= sca * np) {
+      if (np > XXX) {
+        h1 /= np; h2 /= np;
+        if (h1 < 0) h1 = 0;
+        if (h2 > sca) h2 = sca;
+      } else { h1 = 0; h2 = sca; }
+      if (h1 < hi && h2 > sqrtf(XXX) * e.hr) { hi = h1; hf = h2; }
+    }
+  }
+  return make_float2(hi, hf);
+}
+
+struct Truncated {
+  float SCA, TOT, del;
+  int om, J;
+};
+
+// gpu/pro.cu:677-717: a step cut short at fin (DOM hit or hole-ice entry): the optical
+// depths used over the bulk-ice part by layers, then the hole-ice part.
+__device__ __noinline__ Truncated truncated_step(const ppcb_params& e, const float2* __restrict__ wz, float z, float nz,
+                                                 float fin, float edh, int I, int sign, float anz, float SCA,
+                                                 float TOT, float nr, float hi, float hf, float del, float sca,
+                                                 int om) {
+  Truncated t;
+  {
+    float xs = 0, xa = 0;
+    float y = z + nz * fin / edh;
+    const int J = imin(imax(__float2int_rn(y), 0), e.size - 1);
+    t.J = J;
+    if (I == J) { float2 c = ice(wz, I); xs = fin * c.y; xa = fin * c.x; }
+    else {
+      float h = 0.5f - sign * (z - I);
+      float g = 0.5f + sign * (y - J);
+      float2 ci = ice(wz, I), cj = ice(wz, J);
+      xs = h * ci.y + g * cj.y;
+      xa = h * ci.x + g * cj.x;
+      for (int i = I + sign; i != J && (unsigned)i < (unsigned)e.size; i += sign) { float2 c = ice(wz, i); xs += c.y; xa += c.x; }
+      float f = edh / anz;
+      xs *= f; xa *= f;
+    }
+    if (xs < 0) xs = 0;
+    if (xa < 0) xa = 0;
+    SCA -= xs; TOT -= xa;
+  }
+  TOT *= nr;
+  if (hi < del) {
+    float fin2 = fminf(hi + fminf(SCA / e.hs, TOT / e.ha), hf);
+    if (om != -1) { if (fin2 < del) { del = fin2; om = -1; } }
+    else {
+      if (fin2 < del) del = fin2;
+      else del = fminf(fin2, sca);
+    }
+    fin2 = del - hi;
+    SCA -= fin2 * e.hs; TOT -= fin2 * e.ha;
+  }
+  t.SCA = SCA; t.TOT = TOT; t.del = del; t.om = om;
+  return t;
+}
+
+// gpu/pro.cu:728: a step with a non-finite optical depth is counted (and the first four SMs
+// where it happened recorded); the photon is then dropped by the caller
+__device__ __noinline__ void record_nan_step(const KArgs& a) {
+  unsigned int k = atomicAdd(&a.ctrl->nan_steps, 1u);
+  if (k < 4) { unsigned int sm; asm volatile("mov.u32 %0, %%smid;" : "=r"(sm)); a.ctrl->bad_sm[k] = sm; }
+}
 
 // gpu/pro.cu:499-888: one propagation step (one scattering segment).  Returns with
 // ph.TOT == 0 once the photon is absorbed or registered.
@@ -636,19 +717,8 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
           }
         }
         if (hole_on) {  // hole-ice column around the string
-          float DH = b * b - (c - e.hr2) * np;
-          if (DH > 0) {
-            DH = sqrtf(DH);
-            float h1 = b - DH, h2 = b + DH;
-            if (h2 >= 0 && h1 <= sca * np) {
-              if (np > XXX) {
-                h1 /= np; h2 /= np;
-                if (h1 < 0) h1 = 0;
-                if (h2 > sca) h2 = sca;
-              } else { h1 = 0; h2 = sca; }
-              if (h1 < hi && h2 > sqrtf(XXX) * e.hr) { hi = h1; hf = h2; }
-            }
-          }
+          const float2 h = hole_column(e, b, c, np, sca, hi, hf);
+          hi = h.x; hf = h.y;
         }
       }
     }
@@ -656,45 +726,16 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
 
   float fin = fminf(del, hi);
   bool hole = fin < sca;
-  if (hole) {  // truncated step: overburden by layers, hole ice, gpu/pro.cu:677-717
-    {
-      float xs = 0, xa = 0;
-      float y = z + n.z * fin / edh;
-      J = imin(imax(__float2int_rn(y), 0), e.size - 1);
-      if (I == J) { float2 c = ice(wz, I); xs = fin * c.y; xa = fin * c.x; }
-      else {
-        float h = 0.5f - sign * (z - I);
-        float g = 0.5f + sign * (y - J);
-        float2 ci = ice(wz, I), cj = ice(wz, J);
-        xs = h * ci.y + g * cj.y;
-        xa = h * ci.x + g * cj.x;
-        for (int i = I + sign; i != J && (unsigned)i < (unsigned)e.size; i += sign) { float2 c = ice(wz, i); xs += c.y; xa += c.x; }
-        float f = edh / anz;
-        xs *= f; xa *= f;
-      }
-      if (xs < 0) xs = 0;
-      if (xa < 0) xa = 0;
-      SCA -= xs; TOT -= xa;
-    }
-    TOT *= nr;
-    if (hi < del) {
-      float fin2 = fminf(hi + fminf(SCA / e.hs, TOT / e.ha), hf);
-      if (om != -1) { if (fin2 < del) { del = fin2; om = -1; } }
-      else {
-        if (fin2 < del) del = fin2;
-        else del = fminf(fin2, sca);
-      }
-      fin2 = del - hi;
-      SCA -= fin2 * e.hs; TOT -= fin2 * e.ha;
-    }
+  if (hole) {  // truncated step (a DOM or the hole-ice column ends it first): rare, out of line
+    const Truncated t = truncated_step(e, wz, z, n.z, fin, edh, I, sign, anz, SCA, TOT, nr, hi, hf, del, sca, om);
+    SCA = t.SCA; TOT = t.TOT; del = t.del; om = t.om; J = t.J;
   } else { SCA = 0; TOT = tot * nr; }
 
   hk.segment(I, z, sign, anz, edh, nr, fin, n.z, e.size);  // bulk-ice part of the step (the rest is hole ice)
   r.x += del * n.x; r.y += del * n.y; r.z += del * n.z; r.w += del * n.w;
 
   if (!isfinite(TOT) || !isfinite(SCA)) {  // gpu/pro.cu:728
-    unsigned int k = atomicAdd(&a.ctrl->nan_steps, 1u);
-    if (k < 4) { unsigned int sm; asm volatile("mov.u32 %0, %%smid;" : "=r"(sm)); a.ctrl->bad_sm[k] = sm; }
+    record_nan_step(a);
     TOT = 0; om = -1;
     nan_steps++;
   }

@@ -37,9 +37,10 @@ namespace ppcb {
 PPCB_HD int tmin(int a, int b) { return b < a ? b : a; }
 PPCB_HD int tmax(int a, int b) { return a < b ? b : a; }
 
+// 1-d: interpolate between the two maps bracketing the distance along 225 deg
 template <class Tab>
-PPCB_HD float zshift_t(const ppcb_params& d, const Tab& t, float rx, float ry, float rz, float& dz) {
-  if (d.tmod == 1) {  // 1-d: interpolate between the two maps bracketing the distance along 225 deg
+PPCB_HD float zshift_1d_t(const ppcb_params& d, const Tab& t, float rx, float ry, float rz, float& dz) {
+  {
     float nr = PPCB_SUB(PPCB_ADD(PPCB_MUL(d.lnx, rx), PPCB_MUL(d.lny, ry)), d.r0);
     // first j >= 1 with nr < lr[j], or j = lnum-1.  The radii are non-decreasing (checked
     // when loaded), so that is 1 + #{k in [1, lnum-2] : !(nr < lr[k])}: a loop with the same
@@ -62,7 +63,13 @@ PPCB_HD float zshift_t(const ppcb_params& d, const Tab& t, float rx, float ry, f
     float r = PPCB_ADD(qx, PPCB_MUL(qy, PPCB_SUB(z, (float)k)));
     if (d.vthk != 0) dz = PPCB_DIV(dz, PPCB_SUB(1.f, PPCB_MUL(d.lrdz, qy)));
     return r;
-  } else if (d.tmod == 2) {  // 2-d: barycentric interpolation on the skewed map grid
+  }
+}
+
+// 2-d: barycentric interpolation on the skewed map grid
+template <class Tab>
+PPCB_HD float zshift_2d_t(const ppcb_params& d, const Tab& t, float rx, float ry, float rz, float& dz) {
+  {
     float qx = PPCB_ADD(PPCB_MUL(d.cb[0][0], rx), PPCB_MUL(d.cb[1][0], ry));
     float qy = PPCB_ADD(PPCB_MUL(d.cb[0][1], rx), PPCB_MUL(d.cb[1][1], ry));
     qx = PPCB_DIV(PPCB_SUB(qx, d.mmin[0]), d.mstp[0]);
@@ -118,6 +125,12 @@ PPCB_HD float zshift_t(const ppcb_params& d, const Tab& t, float rx, float ry, f
     if (d.vthk != 0) dz = PPCB_DIV(dz, PPCB_SUB(1.f, PPCB_MUL(d.lrdz, ay)));
     return r;
   }
+}
+
+template <class Tab>
+PPCB_HD float zshift_t(const ppcb_params& d, const Tab& t, float rx, float ry, float rz, float& dz) {
+  if (d.tmod == 1) return zshift_1d_t(d, t, rx, ry, rz, dz);
+  if (d.tmod == 2) return zshift_2d_t(d, t, rx, ry, rz, dz);
   return 0;
 }
 
