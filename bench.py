@@ -35,8 +35,9 @@ PHOTONS = 100_000_000
 FCV = math.pi / 180
 
 
-def _cascade_bunch(rng, photons, q=1, ppm=2450.08):
-    """EM cascade bunch with the reference's longitudinal parameters (gpu/f2k.cxx:68-79)."""
+def _cascade_bunch(rng, photons, q=1, ppm=2450.08, fixed=None):
+    """EM cascade bunch with the reference's longitudinal parameters (gpu/f2k.cxx:68-79):
+    random vertex and direction, or `fixed` = (x, y, z, nx, ny, nz)."""
     from ppc_b200 import types as T
     # energy whose mean yield at xR=5 is `photons` propagated photons (gpu/f2k.cxx:68-71,
     # :502): photons = ppm * 5.321*0.910/0.9216 * E / 25
@@ -48,9 +49,11 @@ def _cascade_bunch(rng, photons, q=1, ppm=2450.08):
     ct = rng.uniform(-1, 1)
     ph = rng.uniform(0, 2 * math.pi)
     st = math.sqrt(1 - ct * ct)
-    bunch = T.bunch_particle([v[0], v[1], v[2], 0.0], [st * math.cos(ph), st * math.sin(ph), ct], q, photons,
-                             -11, f=0.0, a=a, b=b)
-    return bunch, E, v
+    d = [st * math.cos(ph), st * math.sin(ph), ct]
+    if fixed is not None:
+        v, d = list(fixed[:3]), list(fixed[3:6])
+    bunch = T.bunch_particle([v[0], v[1], v[2], 0.0], d, q, photons, -11, f=0.0, a=a, b=b)
+    return bunch, E, v, d
 
 
 class Clocks:
@@ -138,19 +141,21 @@ def cpu_reference_sample(photons_per_proc, procs, seed=0):
     return {"value": rate, "photons": photons, "seconds": secs}
 
 
-def plain_kernel_sample(photons, events, local):
+def plain_kernel_sample(cascades, photons, local):
     """The reference's own CUDA kernel (gpu/pro.cu built for sm_100a with gpu/Makefile's
-    flags, oracle/_ref/ref_gpu_harness) on the same cascade workload, one eout() per event;
-    device time from the reference's own CUDA events (gpu/ppc.cu:296-304)."""
+    flags, oracle/_ref/ref_gpu_harness) on the same cascades as the timed steps (vertex,
+    direction, energy), one eout() per cascade; device time from the reference's own CUDA
+    events (gpu/ppc.cu:296-304)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
-    if not os.path.exists(exe):
+    if not os.path.exists(exe) or not cascades:
         return None
     ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
-    E = photons * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
-    spec = f"cascade:12.5:-40:60:{E}:0.6:0:0.8:11"
+    path = os.path.join(tempfile.mkdtemp(), "cascades.txt")
+    with open(path, "w") as f:
+        for v, d, E in cascades:
+            f.write("C %.9g %.9g %.9g %.9g %.9g %.9g %.9g %d\n" % (v[0], v[1], v[2], E, d[0], d[1], d[2], photons))
     env = dict(os.environ, PPCTABLESDIR=ice, CUDA_VISIBLE_DEVICES=str(local))
-    r = subprocess.run([exe, spec, str(photons), str(events), "1"], env=env, capture_output=True, text=True,
-                       timeout=600)
+    r = subprocess.run([exe, "file:" + path, "0", "0", "1"], env=env, capture_output=True, text=True, timeout=600)
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     if r.returncode != 0 or not lines:
         return None
@@ -343,10 +348,39 @@ def run_fit(args, local):
     print(json.dumps(line))
 
 
+def _plain_kernel_events(ev, local, timeout=1800):
+    """The reference's CUDA kernel on the same events, one eout() per event (file mode of
+    oracle/_ref/ref_gpu_harness): events/s over its wall time, which includes the
+    reference's per-event host work."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
+    if not os.path.exists(exe):
+        return None
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    path = os.path.join(tempfile.mkdtemp(), "events.txt")
+    with open(path, "w") as f:
+        for x in ev:
+            if x["type"] > 0:
+                k = int(np.int16(x["u"][3] & 0xFFFF))  # flasher DOM index: string-major, 60 per string
+                f.write(f"F {k // 60 + 1} {k % 60 + 1} {int(x['num'])}\n")
+            else:
+                E = int(x["num"]) * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
+                f.write("C %.9g %.9g %.9g %.9g %.9g %.9g %.9g %d\n" % (x["r"][0], x["r"][1], x["r"][2], E, x["n"][0],
+                                                                       x["n"][1], x["n"][2], int(x["num"])))
+    env = dict(os.environ, PPCTABLESDIR=ice, CUDA_VISIBLE_DEVICES=str(local), FLDR="3960", ELEV="30")
+    r = subprocess.run([exe, "file:" + path, "0", "0", "1"], env=env, capture_output=True, text=True, timeout=timeout)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return None
+    x = json.loads(lines[-1])
+    return {"events_per_s": x["events"] / x["wall_s"], "device_ms": x["device_ms"], "wall_s": x["wall_s"],
+            "photons": x["photons"], "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, one eout() per event"}
+
+
 def run_batched(args, local):
     """4096 events (log-uniform 1e3-1e7 photons; half flashers on random DOMs, 12-fold at
     30 degrees, half cascades) in one graph-replayed launch, against the reference's CUDA
-    kernel propagating the same events one eout() at a time."""
+    kernel propagating the same events one eout() at a time.  `by_decade` repeats the
+    comparison on 512 events per decade of photon count."""
     import torch
     from ppc_b200 import synth
     from ppc_b200 import workloads as W
@@ -387,33 +421,30 @@ def run_batched(args, local):
         "gpu_launches": 3 * args.steps,
         "clocks": clocks,
     }
+    decades = []
+    for lo in (1e3, 1e4, 1e5, 1e6):
+        ed = W.batched_events(oms, n_events=512, lo=lo, hi=10 * lo, seed=int(lo))
+        b.run(ed, 512, hits_per_photon=0.02)  # capture for this size
+        rr = [b.run(ed, 512, hits_per_photon=0.02) for _ in range(3)]
+        t = sum(r["graph_ms"] for r in rr) / 1000.0
+        decades.append({"photons_per_event": [lo, 10 * lo], "events": 512, "events_per_s": 512 * len(rr) / t,
+                        "photons_per_s": float(ed["num"].sum()) * len(rr) / t, "_ev": ed})
     b.close()
     c.close()
     torch.cuda.empty_cache()
     if not args.no_plain_kernel:
-        exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
-        if os.path.exists(exe):
-            path = os.path.join(tempfile.mkdtemp(), "events.txt")
-            with open(path, "w") as f:
-                for e in range(args.events):
-                    x = ev[e]
-                    if x["type"] > 0:
-                        k = int(np.int16(x["u"][3] & 0xFFFF))  # flasher DOM index: string-major, 60 per string
-                        f.write(f"F {k // 60 + 1} {k % 60 + 1} {int(x['num'])}\n")
-                    else:
-                        E = int(x["num"]) * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
-                        f.write("C %f %f %f %f %f %f %f %d\n" % (x["r"][0], x["r"][1], x["r"][2], E, x["n"][0],
-                                                                   x["n"][1], x["n"][2], int(x["num"])))
-            env = dict(os.environ, PPCTABLESDIR=ice, CUDA_VISIBLE_DEVICES=str(local), FLDR="3960", ELEV="30")
-            r = subprocess.run([exe, "file:" + path, "0", "0", "1"], env=env, capture_output=True, text=True,
-                               timeout=1800)
-            lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
-            if r.returncode == 0 and lines:
-                x = json.loads(lines[-1])
-                line["plain_kernel"] = {"events_per_s": x["events"] / x["wall_s"], "device_ms": x["device_ms"],
-                                        "wall_s": x["wall_s"], "photons": x["photons"],
-                                        "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, one eout() per event"}
-                line["speedup_vs_plain_kernel"] = line["value"] / line["plain_kernel"]["events_per_s"]
+        pk = _plain_kernel_events(ev, local)
+        if pk:
+            line["plain_kernel"] = pk
+            line["speedup_vs_plain_kernel"] = line["value"] / pk["events_per_s"]
+        for d in decades:
+            pk = _plain_kernel_events(d["_ev"], local)
+            if pk:
+                d["plain_kernel_events_per_s"] = pk["events_per_s"]
+                d["speedup_vs_plain_kernel"] = d["events_per_s"] / pk["events_per_s"]
+    for d in decades:
+        del d["_ev"]
+    line["by_decade"] = decades
     print(json.dumps(line))
 
 
@@ -478,8 +509,12 @@ def run_ours(args, rank, world, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
+    timed_cascades = []
+
     def step(timed):
-        b, _, _ = _cascade_bunch(rng, photons, q=1, ppm=ppm)
+        b, E, v, d = _cascade_bunch(rng, photons, q=1, ppm=ppm, fixed=args.cascade)
+        if timed:
+            timed_cascades.append((v, d, E))
         d_bunch.copy_(torch.from_numpy(b.view(np.uint8).reshape(-1)))
         d_ctrl.zero_()
         flush.fill_(1)  # evict L2 between timed iterations
@@ -513,7 +548,7 @@ def run_ours(args, rank, world, local):
     # end to end through the host API: bunch upload, launch, hit download
     e2e_times, e2e_hits = [], 0
     for k in range(0 if args.no_e2e else args.warmup + args.steps):
-        b, _, _ = _cascade_bunch(rng, photons, q=1, ppm=ppm)
+        b, E, v, d = _cascade_bunch(rng, photons, q=1, ppm=ppm, fixed=args.cascade)
         if dist:
             td.barrier()
         torch.cuda.synchronize()
@@ -571,11 +606,12 @@ def run_ours(args, rank, world, local):
         del d_hits, flush
         torch.cuda.empty_cache()
         c.close()
-        pk = plain_kernel_sample(photons, 2, local)
+        pk = plain_kernel_sample(timed_cascades, photons, local)
         if pk:
             line["plain_kernel"] = {"value": pk["value"], "unit": "photons/s", "device_ms": pk["device_ms"],
                                     "photons": pk["photons"],
-                                    "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, gpu/Makefile flags",
+                                    "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, gpu/Makefile flags, "
+                                            "the timed steps' cascades, one eout() each",
                                     "speedup": value / pk["value"]}
     if not args.no_gradient:
         if args.no_plain_kernel:
@@ -607,6 +643,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")
     ap.add_argument("--no-gradient", action="store_true", help="skip the ice-gradient evaluation")
+    ap.add_argument("--cascade", type=lambda t: [float(x) for x in t.split(",")], default=None,
+                    help="x,y,z,nx,ny,nz: one fixed cascade for every step instead of random ones (profiling)")
     ap.add_argument("--config", default="cascade", choices=["cascade", "batched", "fit"],
                     help="cascade: the headline workload; batched: 4096 events in one launch; "
                          "fit: L-BFGS ice fit over 1280 events")
