@@ -104,14 +104,15 @@ _BFR = [0.0768, 5.4e5, 2.23, 0.00262, 0.0774, 1.55e6, 2.45, 0.00250, 0.00100, 0.
 
 
 def write(kind, path, count=131072, xR=5):
-    """Writes configuration `kind` (small | full | full2d | small_tilt) into directory `path`."""
+    """Writes configuration `kind` (small | small_tilt | small_hole | full | full2d) into
+    directory `path`."""
     os.makedirs(path, exist_ok=True)
     shutil.copyfile(multipliers_file(count), os.path.join(path, "rnd.txt"))
     with open(os.path.join(path, "icemodel.par"), "w") as f:
         f.write("0.90 0.03\n1.08 0.02\n6950.0 970.0\n6620.0 70.0\n")
     _wv(os.path.join(path, "wv.dat"))
     rng = np.random.default_rng(1)
-    if kind in ("small", "small_tilt"):
+    if kind in ("small", "small_tilt", "small_hole"):
         _geo(os.path.join(path, "geo-f2k"), _hexagon7(), [503.0 - 17.0 * k for k in range(60)])
         # 100 layers of 10 m covering z in [-500, 503]: depth = 1948.07 - z
         dp = 1445.0 + 10.0 * np.arange(100)
@@ -121,7 +122,12 @@ def write(kind, path, count=131072, xR=5):
             for d, b, a in zip(dp, be, ba):
                 f.write(f"{d:.2f} {b:.6f} {a:.6f} 0\n")
         with open(os.path.join(path, "cfg.txt"), "w") as f:
-            f.write(f"{xR}\n1.0\n0\n0.9\n")
+            if kind == "small_hole":
+                # hole-ice column of 8 DOM radii around each string: effective scattering
+                # length 0.5 m, absorption length 100 m, SAM fraction 0.35, g = 0.5
+                f.write(f"{xR}\n1.0\n0\n0.9\n130\n0\n0\n8.0\n0.5\n100.0\n0.35\n0.5\n")
+            else:
+                f.write(f"{xR}\n1.0\n0\n0.9\n")
         with open(os.path.join(path, "as.dat"), "w") as f:
             f.write("1\n1\n")
         if kind == "small_tilt":

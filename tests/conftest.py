@@ -43,6 +43,11 @@ def ice_small_tilt():
     return _ice("small_tilt")
 
 
+@pytest.fixture(scope="session")
+def ice_small_hole():
+    return _ice("small_hole")
+
+
 def have_gpu():
     try:
         import torch

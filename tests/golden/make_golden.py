@@ -9,7 +9,8 @@ oracle/_ref/ref_harness) on the synthetic configurations of ppc_b200/synth.py an
   run_<case>.npz        kernel-level hits, a digest of the phase-1 photon records and the
                         final random-stream state of a fixed-seed propagation
 
-Needs /root/reference (run in the build container):  python tests/golden/make_golden.py
+Needs /root/reference (run in the build container):
+    python tests/golden/make_golden.py [names...]   (configurations / cases; default all)
 """
 import hashlib
 import json
@@ -36,7 +37,9 @@ RUNS = [
     ("full_cascade", "full", "cascade:10:20:-300:2000:0.3:0.4:0.8660254:11", 20000, 7, {}),
     ("full2d_flasher", "full2d", "flasher:40:30", 20000, 7, {}),
     ("small_tilt_led", "small_tilt", "flasher:1:30", 20000, 9, {"FWID": "9.7"}),
+    ("small_hole_point", "small_hole", "point:0:0:0", 20000, 11, {"FWID": "-1", "WFLA": "405"}),
 ]
+KINDS = ("small", "full", "full2d", "small_tilt", "small_hole")
 
 
 def ice(kind):
@@ -59,15 +62,20 @@ def probe_points(n, seed):
     return pos
 
 
-def main():
+def main(only=()):
+    """only: configuration and case names to (re)generate; all when empty."""
     if not O.harness_available():
         raise SystemExit("reference harness missing: make -C oracle ref")
     tmp = tempfile.mkdtemp()
-    for kind in ("small", "full", "full2d", "small_tilt"):
+    for kind in KINDS:
+        if only and kind not in only:
+            continue
         raw = O.harness_tables(ice(kind), tmp)
         with open(os.path.join(HERE, f"tables_{kind}.json"), "w") as f:
             json.dump({k: sha(raw[k]) for k in TABLES}, f, indent=1, sort_keys=True)
     for kind in ("full", "full2d", "small_tilt"):
+        if only and kind not in only:
+            continue
         pos = probe_points(2000, 5)
         fi, fo = os.path.join(tmp, "p.bin"), os.path.join(tmp, "z.bin")
         pos.tofile(fi)
@@ -75,6 +83,8 @@ def main():
         z = np.fromfile(fo, np.float32).reshape(-1, 3)[:, :2]
         np.savez_compressed(os.path.join(HERE, f"zshift_{kind}.npz"), pos=pos, zshift=z)
     for case, kind, spec, photons, seed, env in RUNS:
+        if only and case not in only:
+            continue
         info, hits, pbuf, bunch = O.harness_run(ice(kind), spec, photons, seed, os.path.join(tmp, case), env)
         np.savez_compressed(os.path.join(HERE, f"run_{case}.npz"), hits=hits, bunch=bunch,
                             pbuf_head=pbuf[:256], pbuf_sha=np.frombuffer(sha(pbuf.tobytes()).encode(), np.uint8),
@@ -84,4 +94,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))
