@@ -6,6 +6,8 @@ Finite-difference noise (measured with per-photon streams, 1e9 flasher photons p
 evaluation, relative step 0.03 along all layers): about 0.5% for the absorption direction
 and about 2% for the scattering direction, whose perturbed paths move hits in both
 directions.  The tolerances below are set from those figures."""
+import os
+
 import numpy as np
 import pytest
 
@@ -208,4 +210,72 @@ def test_lbfgs_fit_recovers_absorption(ice_full):
           f"{r['accepted']}/{r['iterations']} steps kept, {r['seconds_per_iteration']:.2f} s/iteration")
     assert r["ll"] > lls[0]
     assert err1 < 0.85 * err0
+    c.close()
+
+
+def _scaled_ice(src, dst, ba_scale):
+    """A copy of ice directory `src` with every layer's absorption (icemodel.dat column 3)
+    scaled by ba_scale."""
+    import shutil
+    shutil.copytree(src, dst)
+    rows = open(os.path.join(src, "icemodel.dat")).read().split("\n")
+    out = []
+    for line in rows:
+        f = line.split()
+        if len(f) >= 3:
+            f[2] = "%.9g" % (float(f[2]) * ba_scale)
+        out.append(" ".join(f))
+    open(os.path.join(dst, "icemodel.dat"), "w").write("\n".join(out))
+
+
+def _reference_cpu_hits(ice, spec, photons, procs, seed0, env):
+    """Kernel-level hits of the reference's own CPU build (oracle/_ref/ref_harness_fm),
+    `procs` processes with distinct seeds sharing `photons`."""
+    import json
+    import subprocess
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness_fm")
+    e = dict(os.environ, PPCTABLESDIR=ice, PPCB_QUIET="1", **env)
+    ps = [subprocess.Popen([exe, "run", spec, str(photons // procs), str(seed0 + k), "/tmp/ppcb_fd", "nodump"], env=e,
+                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for k in range(procs)]
+    hits = 0
+    for p in ps:
+        out, _ = p.communicate()
+        hits += json.loads([l for l in out.splitlines() if l.startswith("{")][-1])["hits"]
+    return hits, procs * (photons // procs)
+
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_harness_fm")),
+                    reason="reference CPU build not present")
+def test_gradient_agrees_with_reference_cpu_finite_differences(ice_full, tmp_path):
+    """The adjoint's derivative of the expected hit count along all absorption coefficients
+    (d/dt of N at ba x (1 + t)) against a central difference of the reference's own CPU
+    build (gpu/ppc.cu compiled with its flags) at t = +-0.1, one flasher (string 21, DOM 30,
+    12-fold LEDs at 30 degrees), 6e7 photons per side on the host cores.  The CPU side has
+    no common random numbers, so the tolerance is 3.5 Poisson standard deviations plus 3%
+    for the curvature of exp(-absorption) over the step."""
+    h = 0.1
+    k = 20 * 60 + 29
+    cpus = max(1, min(32, os.cpu_count() or 1))
+    env = {"FLDR": "3960", "ELEV": "30", "FWID": "9.7"}
+    n_ref = 60_000_000
+    plus, minus = str(tmp_path / "plus"), str(tmp_path / "minus")
+    _scaled_ice(ice_full, plus, 1 + h)
+    _scaled_ice(ice_full, minus, 1 - h)
+    hp, n1 = _reference_cpu_hits(plus, "flasher:21:30", n_ref, cpus, 100, env)
+    hm, n2 = _reference_cpu_hits(minus, "flasher:21:30", n_ref, cpus, 200, env)
+    fd = (hp - hm) / (2 * h) / n1
+    sigma = np.sqrt(hp + hm) / (2 * h) / n1
+    c = _ctx(ice_full)
+    be0, ba0 = c.get_ice()
+    oms = c.tables()["oms"]
+    b = W.flasher(k, oms["r"][k], 200_000_000, q=0)
+    r = c.gradient(b, weights=np.ones(c.info()["gsize"], np.float32), hit_cap=2_000_000)
+    adj = float(np.dot(r["g_ba"], ba0)) / 200_000_000
+    print(f"dN/dt per photon: adjoint {adj:.4e}, reference CPU central difference {fd:.4e} +- {sigma:.1e} "
+          f"({hp} / {hm} hits of {n1} photons per side, {cpus} processes)")
+    assert np.sign(adj) == np.sign(fd)
+    assert abs(adj - fd) <= 3.5 * sigma + 0.03 * abs(fd), (adj, fd, sigma)
     c.close()
