@@ -602,7 +602,9 @@ def run_ours(args, rank, world, local):
                              "peak_gbs": _peaks().get("hbm_gbs"), "peak_source": "of measured (MEASURED_PEAKS.json)"}},
         "clocks": clocks,
     }
-    if not args.no_plain_kernel:
+    # the comparisons below are single-GPU figures: a multi-GPU run reports throughput only
+    single = world == 1
+    if single and not args.no_plain_kernel:
         del d_hits, flush
         torch.cuda.empty_cache()
         c.close()
@@ -613,13 +615,13 @@ def run_ours(args, rank, world, local):
                                     "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, gpu/Makefile flags, "
                                             "the timed steps' cascades, one eout() each",
                                     "speedup": value / pk["value"]}
-    if not args.no_gradient:
+    if single and not args.no_gradient:
         if args.no_plain_kernel:
             del d_hits, flush
             torch.cuda.empty_cache()
             c.close()
         line["gradient"] = gradient_sample(local, plain_kernel=not args.no_plain_kernel)
-    if not args.no_cpu_baseline:
+    if single and not args.no_cpu_baseline:
         r = cpu_reference_sample(args.ref_photons, os.cpu_count() or 1)
         if r:
             line["cpu_baseline"] = {"value": r["value"], "unit": "photons/s", "cores": os.cpu_count(),
