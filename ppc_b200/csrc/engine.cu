@@ -205,6 +205,8 @@ void Engine::free_device(DeviceCtx& g) {
 
 void Engine::fin() {
   if (!inited_) return;
+  if (!devs.empty()) cudaSetDevice(devs[0].dev);
+  gs_.reset();
   for (auto& g : devs) free_device(g);
   queue_.clear();
   inited_ = false;

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <deque>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -67,6 +68,8 @@ struct DeviceCtx {
   uint64_t hhits_cap = 0;
 };
 
+struct GradScratch;  // the gradient's device buffers (gradient.cu), kept between calls
+
 class Engine {
  public:
   ~Engine();
@@ -120,6 +123,7 @@ class Engine {
 
  private:
   void free_device(DeviceCtx& g);
+  std::shared_ptr<GradScratch> gs_;  // grows to the largest gradient call; freed by fin()
   bool inited_ = false;
   bool initialized_ = false;
   std::deque<long> queue_;

@@ -20,13 +20,46 @@ void Engine::set_ice(const float* be, const float* ba) {
 }
 
 namespace {
+// device buffer that keeps its memory between calls and grows when a call needs more
 template <class T>
 struct DBuf {
   T* p = nullptr;
-  explicit DBuf(size_t n) { check(cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T)), "gradient buffer"); }
+  size_t cap = 0;
+  void need(size_t n) {
+    n = std::max<size_t>(n, 1);
+    if (n <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    check(cudaMalloc((void**)&p, n * sizeof(T)), "gradient buffer");
+    cap = n;
+  }
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { if (p) cudaFree(p); }
 };
 }  // namespace
+
+struct GradScratch {
+  DBuf<ppcb_bunch> bunches;
+  DBuf<uint64_t> bstart;
+  DBuf<ppcb_hit> hits;
+  DBuf<unsigned char> prov;
+  DBuf<ppcb_ctrl> ctrl;
+  DBuf<unsigned int> counts;
+  DBuf<float> weights;
+  DBuf<float2> wgrad;
+  DBuf<double> g;
+  DBuf<unsigned int> stats;
+  cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+  GradScratch() {
+    for (auto& x : e) check(cudaEventCreate(&x), "event");
+  }
+  ~GradScratch() {
+    for (auto& x : e) if (x) cudaEventDestroy(x);
+  }
+};
 
 Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, const float* observed,
                               const float* weights, double scale, uint64_t hit_cap) {
@@ -39,16 +72,28 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, cons
   const size_t nbins = (size_t)gsize * (events ? events : 1);  // charge bins: DOM, or (event, DOM)
   std::vector<uint64_t> bs(nb + 1, 0);
   for (int k = 0; k < nb; k++) bs[k + 1] = bs[k] + b[k].num;
-  DBuf<ppcb_bunch> db(nb);
-  DBuf<uint64_t> dbs(nb + 1);
-  DBuf<ppcb_hit> dh(hit_cap);
-  DBuf<unsigned char> dprov(hit_cap * kProvBytes);
-  DBuf<ppcb_ctrl> dctrl(1);
-  DBuf<unsigned int> dcnt(nbins);
-  DBuf<float> dw(nbins);
-  DBuf<float2> dwg(PPCB_WNUM);
-  DBuf<double> dgo(2 * PPCB_MAXLYS);
-  DBuf<unsigned int> dstat(2);
+  if (!gs_) gs_ = std::make_shared<GradScratch>();
+  GradScratch& X = *gs_;
+  X.bunches.need(nb);
+  X.bstart.need(nb + 1);
+  X.hits.need(hit_cap);
+  X.prov.need(hit_cap * kProvBytes);
+  X.ctrl.need(1);
+  X.counts.need(nbins);
+  X.weights.need(nbins);
+  X.wgrad.need(PPCB_WNUM);
+  X.g.need(2 * PPCB_MAXLYS);
+  X.stats.need(2);
+  auto& db = X.bunches;
+  auto& dbs = X.bstart;
+  auto& dh = X.hits;
+  auto& dprov = X.prov;
+  auto& dctrl = X.ctrl;
+  auto& dcnt = X.counts;
+  auto& dw = X.weights;
+  auto& dwg = X.wgrad;
+  auto& dgo = X.g;
+  auto& dstat = X.stats;
   cudaStream_t st = g.st;
   check(cudaMemcpyAsync(db.p, b, nb * sizeof(ppcb_bunch), cudaMemcpyHostToDevice, st), "H2D bunches");
   check(cudaMemcpyAsync(dbs.p, bs.data(), (nb + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "H2D offsets");
@@ -57,10 +102,7 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, cons
   check(cudaMemsetAsync(dcnt.p, 0, nbins * sizeof(unsigned int), st), "memset");
   check(cudaMemsetAsync(dgo.p, 0, 2 * PPCB_MAXLYS * sizeof(double), st), "memset");
   check(cudaMemsetAsync(dstat.p, 0, 2 * sizeof(unsigned int), st), "memset");
-  cudaEvent_t e0, e1, e2;
-  check(cudaEventCreate(&e0), "event");
-  check(cudaEventCreate(&e1), "event");
-  check(cudaEventCreate(&e2), "event");
+  cudaEvent_t e0 = X.e[0], e1 = X.e[1], e2 = X.e[2];
   // recording forward pass
   KArgs a = args_for(0);
   a.bunches = db.p; a.bstart = dbs.p; a.nb = nb; a.num = bs[nb];
@@ -108,9 +150,6 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, cons
   check(cudaStreamSynchronize(st), "replay");
   check(cudaEventElapsedTime(&out.forward_ms, e0, e1), "elapsed");
   check(cudaEventElapsedTime(&out.backward_ms, e1, e2), "elapsed");
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(e2);
   // kernel layers run from the deepest row of icemodel.dat (layer i <-> row size-1-i)
   out.g_be.assign(size, 0.0);
   out.g_ba.assign(size, 0.0);
