@@ -227,6 +227,41 @@ def gradient_sample(local, events=64, photons=10_000_000, steps=3, plain_kernel=
                                       "kind": "central differences, 2 x 342 forward runs of the reference CUDA "
                                               "kernel (gpu/pro.cu, sm_100a), one eout() per event"}
             out["speedup_vs_fd_plain_kernel"] = out["evals_per_s"] * fd_s
+    # the same 64 flasher events through the drop-in API (llh/ppc.h semantics: flset, sett,
+    # flone, eout with the host back end, hitz, efin), wall time, against the reference's
+    # own host code doing the same (the plain-kernel forward above)
+    old = {k: os.environ.get(k) for k in ("FLDR", "ELEV")}
+    os.environ.update(FLDR="3960", ELEV="30")
+    try:
+        c = PPC()
+        c.initialize(1.0, ice)
+        c.set_seed(4243)
+        c.choose(local)
+        c.ini()
+        kept = 0
+        for rep in range(2):  # the first pass warms up
+            t0 = time.perf_counter()
+            for e, k in enumerate(doms):
+                c.flset(int(k) // 60 + 1, int(k) % 60 + 1)
+                c.sett(0.0, 0.0, 1.0, (e, 0), 0)
+                c.flone(photons)
+                c.eout()
+                kept += len(c.hitz())
+                c.efin()
+            wall = time.perf_counter() - t0
+        c.close()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    x = {"events": events, "photons": events * photons, "wall_s": wall, "hitz_records": kept // 2,
+         "kind": "flset/sett/flone/eout/hitz/efin per event, the reference's host back end included"}
+    if "fd_plain_kernel" in out:
+        x["reference_wall_s"] = out["fd_plain_kernel"]["forward_wall_s"]
+        x["speedup"] = x["reference_wall_s"] / wall
+    out["xppc_e2e"] = x
     return out
 
 

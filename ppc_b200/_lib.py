@@ -50,10 +50,11 @@ class Dom(C.Structure):
     _fields_ = [("R", C.c_float), ("F", C.c_float), ("r", C.c_float * 3)]
 
 
+# ppcb_hitz_rec: 76 bytes of fields, padded to 80 by the C compiler (8-byte alignment)
 HITZ_DTYPE = __import__("numpy").dtype([
     ("track_first", "<i4"), ("frame", "<i4"), ("track_second", "<u8"), ("t0", "<f8"),
     ("str", "<i4"), ("om", "<i4"), ("pmt", "<i4"), ("dir", "<f4"), ("time", "<f4"),
-    ("r", "<f4", 4), ("n", "<f4", 4)])
+    ("r", "<f4", 4), ("n", "<f4", 4), ("pad_", "<u4")])
 
 # exported C symbols (kept in sync with include/ppc_b200.h; tests check every one loads)
 EXPORTS = [

@@ -183,3 +183,45 @@ def test_gradient_checks_charge_bin_sizes(ice_small):
         c.gradient(b, weights=np.zeros((3, gs), np.float32), events=3)
     assert e.value.code == 6
     c.close()
+
+
+def test_record_layouts_match_the_c_header(tmp_path):
+    """Every record the Python side exchanges with the C ABI has the C compiler's size and
+    field offsets (a mismatch makes a copy-out call overrun the Python buffer)."""
+    from ppc_b200 import types as T
+    src = tmp_path / "sz.c"
+    src.write_text("""
+#include <stdio.h>
+#include <stddef.h>
+#include "ppc_b200.h"
+#define F(t, m) printf(#t "." #m " %zu\\n", offsetof(t, m))
+int main(void) {
+  printf("ppcb_hitz_rec %zu\\n", sizeof(ppcb_hitz_rec));
+  printf("ppcb_hit %zu\\n", sizeof(ppcb_hit));
+  printf("ppcb_bunch %zu\\n", sizeof(ppcb_bunch));
+  printf("ppcb_run_info %zu\\n", sizeof(ppcb_run_info));
+  printf("ppcb_info %zu\\n", sizeof(ppcb_info));
+  printf("ppcb_batch_info %zu\\n", sizeof(ppcb_batch_info));
+  printf("ppcb_tune_info %zu\\n", sizeof(ppcb_tune_info));
+  printf("ppcb_grad_info %zu\\n", sizeof(ppcb_grad_info));
+  printf("ppcb_ctrl %zu\\n", sizeof(ppcb_ctrl));
+  printf("ppcb_params %zu\\n", sizeof(ppcb_params));
+  F(ppcb_hitz_rec, t0); F(ppcb_hitz_rec, str); F(ppcb_hitz_rec, r); F(ppcb_hitz_rec, n);
+  return 0;
+}
+""")
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    c = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                      check=True).stdout.splitlines())
+    import ctypes as C
+    py = {"ppcb_hitz_rec": _lib.HITZ_DTYPE.itemsize, "ppcb_hit": T.HIT_DTYPE.itemsize,
+          "ppcb_bunch": T.BUNCH_DTYPE.itemsize, "ppcb_run_info": C.sizeof(_lib.RunInfo),
+          "ppcb_info": C.sizeof(_lib.Info), "ppcb_batch_info": C.sizeof(_lib.BatchInfo),
+          "ppcb_tune_info": C.sizeof(_lib.TuneInfo), "ppcb_grad_info": C.sizeof(_lib.GradInfo),
+          "ppcb_ctrl": C.sizeof(T.Ctrl), "ppcb_params": C.sizeof(T.Params)}
+    for k, v in py.items():
+        assert int(c[k]) == v, (k, c[k], v)
+    d = _lib.HITZ_DTYPE
+    for f in ("t0", "str", "r", "n"):
+        assert int(c[f"ppcb_hitz_rec.{f}"]) == d.fields[f][1], f

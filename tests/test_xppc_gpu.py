@@ -1,0 +1,94 @@
+"""The drop-in path end to end on the GPU: the reference's library API (llh/ppc.h
+semantics: flset, sett, flone, eout, hitz, efin) from Python and from a C++ program linked
+against libxppc.so, with the host back end (acceptance, PMT assignment, time binning)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import have_gpu
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_gpu(), reason="needs a CUDA GPU")]
+
+from ppc_b200.api import PPC  # noqa: E402
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_eout_fills_hitz_with_accepted_hits(ice_full, monkeypatch):
+    monkeypatch.setenv("FLDR", "3960")
+    monkeypatch.setenv("ELEV", "30")
+    c = PPC()
+    c.initialize(1.0, ice_full)
+    c.set_seed(21)
+    c.choose(0)
+    c.ini()
+    c.keep_raw(True)
+    c.set_res(10.0)  # 10 ns time bins
+    total, nraw = 0, 0
+    for e, (s, om) in enumerate([(21, 30), (45, 36), (60, 10)]):
+        c.flset(s, om)
+        c.sett(0.0, 0.0, 1.0, (e, 7), 0)
+        c.flone(5_000_000)
+        c.eout()
+        h = c.hitz()
+        assert len(h) > 0
+        assert set(h["track_first"]) == {e} and set(h["track_second"]) == {7}
+        assert h["str"].min() >= 1 and h["str"].max() <= 86 and h["om"].min() >= 1 and h["om"].max() <= 60
+        assert np.allclose(h["time"] / 10.0 - np.floor(h["time"] / 10.0), 0.5)  # bin centres
+        assert np.all(np.isfinite(h["r"])) and np.all(np.isfinite(h["n"]))
+        assert np.allclose(np.linalg.norm(h["n"][:, :3], axis=1), 1, atol=1e-4)
+        raw = c.raw_hits()
+        assert set(raw["n"]) == {e + 1}  # this event's segment
+        assert len(h) <= len(raw)  # acceptance keeps a fraction of the kernel-level hits
+        total += len(h)
+        nraw += len(raw)
+        c.efin()  # clears the event's hit map and kernel-level hits
+        assert len(c.hitz()) == 0 and len(c.raw_hits()) == 0
+    assert 0 < total < nraw
+    last, tot = c.last_run()
+    assert tot["photons"] > 0 and tot["hits"] >= nraw
+    c.close()
+
+
+LLH_LIKE = r"""
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <vector>
+#include "xppc.h"
+int main() {
+  xppc::start();
+  xppc::initialize(1.f);
+  xppc::choose(0);
+  xppc::ini();
+  xppc::flset(21, 30);
+  xppc::sett(0, 0, 1, std::make_pair(3, 9ULL), 0);
+  xppc::flone(4000000);
+  xppc::eout();
+  size_t n = 0;
+  for (xppc::outz::const_iterator i = xppc::hitz.begin(); i != xppc::hitz.end(); ++i) n += i->second.size();
+  printf("hitz %zu\n", n);
+  xppc::efin();
+  xppc::fin();
+  printf("device %g\n", xppc::getTotalDeviceTime());
+  xppc::stop();
+  return n > 0 ? 0 : 1;
+}
+"""
+
+
+def test_program_linked_against_libxppc_runs(ice_full, tmp_path):
+    lib = os.path.join(ROOT, "ppc_b200", "lib")
+    src = tmp_path / "llh_like.cxx"
+    src.write_text(LLH_LIKE)
+    exe = tmp_path / "llh_like"
+    r = subprocess.run(["g++", "-O1", "-std=c++11", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L" + lib, "-lxppc", "-Wl,-rpath," + lib], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    env = dict(os.environ, PPCTABLESDIR=ice_full, FLDR="3960", ELEV="30")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, (r.stdout[-500:], r.stderr[-2000:])
+    n = int([l for l in r.stdout.splitlines() if l.startswith("hitz")][0].split()[1])
+    assert n > 100
