@@ -238,17 +238,22 @@ def gradient_sample(local, events=64, photons=10_000_000, steps=3, plain_kernel=
         c.set_seed(4243)
         c.choose(local)
         c.ini()
+        inf = c.info()
+        # flone(n) propagates n x (ppm / 2450.08) / xR^2 photons (gpu/f2k.cxx:586-588)
+        nsrc = int(round(photons * inf["ovr"] * 2450.08 / inf["eff"]))
         kept = 0
         for rep in range(2):  # the first pass warms up
+            p0 = c.last_run()[1]["photons"]
             t0 = time.perf_counter()
             for e, k in enumerate(doms):
                 c.flset(int(k) // 60 + 1, int(k) % 60 + 1)
                 c.sett(0.0, 0.0, 1.0, (e, 0), 0)
-                c.flone(photons)
+                c.flone(nsrc)
                 c.eout()
                 kept += len(c.hitz())
                 c.efin()
             wall = time.perf_counter() - t0
+            propagated = c.last_run()[1]["photons"] - p0
         c.close()
     finally:
         for k, v in old.items():
@@ -256,11 +261,14 @@ def gradient_sample(local, events=64, photons=10_000_000, steps=3, plain_kernel=
                 os.environ.pop(k, None)
             else:
                 os.environ[k] = v
-    x = {"events": events, "photons": events * photons, "wall_s": wall, "hitz_records": kept // 2,
+    x = {"events": events, "photons": propagated, "wall_s": wall, "photons_per_s": propagated / wall,
+         "hitz_records": kept // 2,
          "kind": "flset/sett/flone/eout/hitz/efin per event, the reference's host back end included"}
     if "fd_plain_kernel" in out:
-        x["reference_wall_s"] = out["fd_plain_kernel"]["forward_wall_s"]
-        x["speedup"] = x["reference_wall_s"] / wall
+        rw = out["fd_plain_kernel"]["forward_wall_s"]
+        x["reference_photons_per_s"] = events * photons / rw
+        x["reference_wall_s"] = rw
+        x["speedup"] = x["photons_per_s"] / x["reference_photons_per_s"]
     out["xppc_e2e"] = x
     return out
 
