@@ -154,7 +154,7 @@ class PPC:
     def propagate(self, bunches, cap=1 << 22):
         """Host bunches in, kernel-level hits out (copies included)."""
         bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
-        hits = np.zeros(cap, T.HIT_DTYPE)
+        hits = np.empty(cap, T.HIT_DTYPE)  # only the first min(produced, cap) records are written
         nh = C.c_uint64()
         info = RunInfo()
         check(lib().ppcb_propagate(self._c, _p(bunches), len(bunches), _p(hits), cap, C.byref(nh), C.byref(info)))
