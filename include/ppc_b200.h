@@ -229,6 +229,22 @@ int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t e
 int ppcb_propagate_noalloc(ppcb_ctx* c, int device, const ppcb_bunch* bunches, int32_t nb, uint64_t num,
                            ppcb_hit* hits, uint64_t hcap, uint64_t* nhits, void* stream);
 
+/* ---- hit back end on the device ----
+ * The reference's back end runs on the host inside eout() (gpu/f2k.cxx:247-363); these
+ * apply the same acceptance to kernel-level hits on the GPU: the wavelength x RDE
+ * acceptance of the DOM's (module type, variant), the sensor's angular acceptance (standard
+ * sensors; others are rejected with PPCB_EARG), the cable shadow, and a wavelength sampled
+ * in the hit's bin.  Each hit draws from its own random stream keyed by (seed, hit index)
+ * instead of the host's shared sequence: the same decisions in distribution, not hit by
+ * hit.  Accepted hits are written in input order.
+ * ppcb_accept_device: device pointers on `stream`; *count (a device pointer) receives the
+ * number accepted; `out` must hold n records.  ppcb_accept: host buffers, device 0; at most
+ * `cap` records written, *nout receives the number accepted. */
+int ppcb_accept_device(ppcb_ctx* c, int device, const ppcb_hit* hits, uint64_t n, uint32_t seed, ppcb_acc_hit* out,
+                       unsigned long long* count, void* stream);
+int ppcb_accept(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n, uint32_t seed, ppcb_acc_hit* out, uint64_t cap,
+                uint64_t* nout);
+
 /* ---- measurement ----
  * No counterpart in the reference.  FP32 FMA throughput of `device` (TFLOP/s, best of
  * `repeats` launches of an FFMA loop over every SM): the denominator of the propagation

@@ -66,7 +66,7 @@ EXPORTS = [
     "ppcb_rng_reset", "ppcb_table", "ppcb_generate_device", "ppcb_index_probe_device", "ppcb_propagate_noalloc",
     "ppcb_batch_create", "ppcb_batch_destroy", "ppcb_batch_set_graph", "ppcb_batch_run", "ppcb_batch_counts",
     "ppcb_batch_hits", "ppcb_batch_autotune", "ppcb_set_ice", "ppcb_get_ice", "ppcb_gradient",
-    "ppcb_fp32_peak",
+    "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept",
 ]
 
 
@@ -128,6 +128,8 @@ def lib():
         "ppcb_get_ice": (i32, [vp, vp, vp, P(i32)]),
         "ppcb_gradient": (i32, [vp, vp, i32, u32, vp, vp, f64, u64, vp, vp, vp, P(GradInfo)]),
         "ppcb_fp32_peak": (i32, [i32, i32, P(f64), P(f64)]),
+        "ppcb_accept_device": (i32, [vp, i32, vp, u64, u32, vp, vp, vp]),
+        "ppcb_accept": (i32, [vp, vp, u64, u32, vp, u64, P(u64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -321,3 +321,17 @@ def fp32_peak(device=0, repeats=5):
     t, ms = C.c_double(), C.c_double()
     check(lib().ppcb_fp32_peak(int(device), int(repeats), C.byref(t), C.byref(ms)))
     return t.value
+
+
+def _accept(self, hits, seed=0):
+    """Device hit back end (ppcb_accept): the acceptance of the reference's host back end
+    applied on the GPU, one random stream per hit.  Returns the accepted hits (ACC_DTYPE)
+    in input order; `hit` indexes the input."""
+    hits = np.ascontiguousarray(hits, T.HIT_DTYPE)
+    out = np.empty(max(1, len(hits)), T.ACC_DTYPE)
+    n = C.c_uint64()
+    check(lib().ppcb_accept(self._c, _p(hits), len(hits), int(seed) & 0xFFFFFFFF, _p(out), len(out), C.byref(n)))
+    return out[:n.value]
+
+
+PPC.accept = _accept

@@ -33,7 +33,7 @@ NVFLAGS = ARCH + ["-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-Xcompil
 CXXFLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-result",
             "-I" + os.path.join(CUDA_HOME, "include"), "-I" + INC]
 
-CU = ["propagate.cu", "engine.cu", "noalloc.cu", "batch.cu", "gradient.cu", "peak.cu"]
+CU = ["propagate.cu", "engine.cu", "noalloc.cu", "batch.cu", "gradient.cu", "peak.cu", "backend.cu"]
 CPP = ["config.cpp", "session.cpp", "capi.cpp", "capi_batch.cpp", "xppc.cpp"]
 CLI = ["ppc_cli.cpp"]
 HEADERS = ["ppcb_types.h", "config.h", "engine.h", "propagate.cuh", "session.h", "ctx.h", "tilt.h", "batch.h"]

@@ -148,3 +148,50 @@ int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t e
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int ppcb_accept_device(ppcb_ctx* c, int device, const ppcb_hit* hits, uint64_t n, uint32_t seed, ppcb_acc_hit* out,
+                       unsigned long long* count, void* stream) {
+  if (!c || (n > 0 && (!hits || !out)) || !count) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    if (device < 0 || device >= (int)c->s.eng.devs.size()) throw ppcb::Error("bad device index", PPCB_EARG);
+    c->s.eng.accept(device, hits, n, seed, out, count, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int ppcb_accept(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n, uint32_t seed, ppcb_acc_hit* out, uint64_t cap,
+                uint64_t* nout) {
+  if (!c || (n > 0 && !hits) || !nout) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    ppcb::Engine& e = c->s.eng;
+    if (!e.ready()) throw ppcb::Error("ppcb_ini() must come before the back end", PPCB_ESTATE);
+    ppcb::check(cudaSetDevice(e.devs[0].dev), "cudaSetDevice");
+    ppcb_hit* dh = nullptr;
+    ppcb_acc_hit* dout = nullptr;
+    unsigned long long* dcnt = nullptr;
+    auto release = [&]() {
+      if (dh) cudaFree(dh);
+      if (dout) cudaFree(dout);
+      if (dcnt) cudaFree(dcnt);
+    };
+    try {
+      ppcb::check(cudaMalloc((void**)&dh, std::max<uint64_t>(n, 1) * sizeof(ppcb_hit)), "back end input");
+      ppcb::check(cudaMalloc((void**)&dout, std::max<uint64_t>(n, 1) * sizeof(ppcb_acc_hit)), "back end output");
+      ppcb::check(cudaMalloc((void**)&dcnt, sizeof(unsigned long long)), "back end count");
+      if (n) ppcb::check(cudaMemcpy(dh, hits, n * sizeof(ppcb_hit), cudaMemcpyHostToDevice), "H2D hits");
+      e.accept(0, dh, n, seed, dout, dcnt, 0);
+      unsigned long long k = 0;
+      ppcb::check(cudaMemcpy(&k, dcnt, sizeof(k), cudaMemcpyDeviceToHost), "D2H count");
+      const uint64_t w = std::min<uint64_t>(k, cap);
+      if (w && out) ppcb::check(cudaMemcpy(out, dout, w * sizeof(ppcb_acc_hit), cudaMemcpyDeviceToHost), "D2H");
+      *nout = k;
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+  });
+}
+
+}  // extern "C"

@@ -27,6 +27,8 @@ struct RunInfo {
   bool overflow = false;
 };
 
+struct BackendTables;  // the device back end's sensor tables (backend.cu)
+
 struct DeviceCtx {
   int dev = -1;
   cudaDeviceProp prop{};
@@ -66,6 +68,7 @@ struct DeviceCtx {
   double device_ms = 0;
   ppcb_hit* hhits = nullptr;       // pinned, grows
   uint64_t hhits_cap = 0;
+  std::shared_ptr<BackendTables> back;  // built on the first device back-end call
 };
 
 struct GradScratch;  // the gradient's device buffers (gradient.cu), kept between calls
@@ -75,7 +78,7 @@ class Engine {
   ~Engine();
   Config cfg;
   unsigned int sv = 0;             // seed: MWC stream start and host rand_r state
-  int deterministic = 0;           // 0 dynamic photon order, 1 static order, 2 static + per-photon streams
+  int deterministic = 0;           // 0 dynamic order, 1 static order (thread streams), 2 dynamic + per-photon streams
   uint32_t max_steps = 1000000;     // per-photon step cap (typical photons take 20-100 steps)
   std::vector<DeviceCtx> devs;
   uint64_t pmax = 0, pmxo = 0;     // photons / bunches per launch
@@ -118,11 +121,17 @@ class Engine {
   // forward launch over the bunches (device 0) and one replay of the recorded hits.
   Grad gradient(const ppcb_bunch* b, int nb, uint32_t events, const float* observed, const float* weights,
                 double scale, uint64_t hit_cap);
+  // Hit back end on device `d` (gpu/f2k.cxx:247-363 acceptance, one random stream per hit):
+  // accepted hits of dhits[0..n) written to dout in input order, their number to *dcount
+  // (device pointer), on stream st.  Standard sensors only.
+  void accept(int d, const ppcb_hit* dhits, uint64_t n, uint32_t seed, ppcb_acc_hit* dout,
+              unsigned long long* dcount, cudaStream_t st);
   double total_device_ms() const;
   KArgs args_for(int d) const;
 
  private:
   void free_device(DeviceCtx& g);
+  void accept_tables(int d);
   std::shared_ptr<GradScratch> gs_;  // grows to the largest gradient call; freed by fin()
   bool inited_ = false;
   bool initialized_ = false;

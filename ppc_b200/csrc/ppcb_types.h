@@ -51,6 +51,20 @@ typedef struct ppcb_hit {
   float dth, dph; // impact point direction seen from the DOM centre
 } ppcb_hit;
 
+// A hit accepted by the back end (gpu/f2k.cxx:247-363): the sensor and PMT it registers
+// on, its time and sampled wavelength, and the two vectors of the reference's hit map
+// record (pout): the impact point relative to the sensor centre and the photon direction.
+typedef struct ppcb_acc_hit {
+  uint32_t i;      // DOM index
+  uint32_t n;      // segment (event) id
+  uint32_t hit;    // index of the kernel-level hit it came from
+  int32_t str, om, pmt;
+  float t;         // time [ns]
+  float wv;        // wavelength [nm]
+  float r[3];      // impact point [m], relative to the sensor centre
+  float d[3];      // photon direction
+} ppcb_acc_hit;
+
 // One photon bunch: `num` photons sharing a source description.
 // type>0: flasher/LED (ka,up,fldr,fla,ofla valid); type<=0: particle (a,b,beta,tau valid).
 typedef struct ppcb_bunch {

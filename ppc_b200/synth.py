@@ -154,9 +154,24 @@ def write(kind, path, count=131072, xR=5):
         f.write("1.0\n0.35\n0.5\n0.15\n")
     if kind == "full2d":
         _tilt2d(path)
+        _sensor_axes_and_cables(path, np.random.default_rng(7))
     else:
         _tilt1d(path, rng)
     return path
+
+
+def _sensor_axes_and_cables(path, rng):
+    """cx.dat: each DOM's axis, a few degrees off vertical (string om nx ny nz r);
+    dx.dat: each DOM's cable azimuth in degrees (string om azimuth r)."""
+    rows = [ln.split() for ln in open(os.path.join(path, "geo-f2k")) if ln.strip()]
+    keys = [(int(r[5]), int(r[6])) for r in rows]
+    with open(os.path.join(path, "cx.dat"), "w") as f:
+        for s, om in keys:
+            nx, ny = rng.normal(0.0, 0.03, 2)
+            f.write(f"{s} {om} {nx:.6f} {ny:.6f} {np.sqrt(1.0 - nx * nx - ny * ny):.6f} 0.5\n")
+    with open(os.path.join(path, "dx.dat"), "w") as f:
+        for s, om in keys:
+            f.write(f"{s} {om} {rng.uniform(-180.0, 180.0):.3f} 1.0\n")
 
 
 def _tilt_shift(depth, r):

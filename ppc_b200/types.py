@@ -52,6 +52,10 @@ class Ctrl(C.Structure):
 HIT_DTYPE = np.dtype([("i", "<u4"), ("n", "<u4"), ("z", "<u4"), ("t", "<f4"),
                       ("pth", "<f4"), ("pph", "<f4"), ("dth", "<f4"), ("dph", "<f4")])
 
+# hit accepted by the back end (ppcb_acc_hit), 56 bytes
+ACC_DTYPE = np.dtype([("i", "<u4"), ("n", "<u4"), ("hit", "<u4"), ("str", "<i4"), ("om", "<i4"), ("pmt", "<i4"),
+                      ("t", "<f4"), ("wv", "<f4"), ("r", "<f4", 3), ("d", "<f4", 3)])
+
 # photon bunch, 64 bytes; the 16-byte union is exposed both ways
 BUNCH_DTYPE = np.dtype([("r", "<f4", 4), ("n", "<f4", 4), ("q", "<u4"), ("num", "<u4"),
                         ("type", "<i4"), ("f", "<f4"), ("u", "<u4", 4)])

@@ -206,6 +206,7 @@ int main(void) {
   printf("ppcb_grad_info %zu\\n", sizeof(ppcb_grad_info));
   printf("ppcb_ctrl %zu\\n", sizeof(ppcb_ctrl));
   printf("ppcb_params %zu\\n", sizeof(ppcb_params));
+  printf("ppcb_acc_hit %zu\\n", sizeof(ppcb_acc_hit));
   F(ppcb_hitz_rec, t0); F(ppcb_hitz_rec, str); F(ppcb_hitz_rec, r); F(ppcb_hitz_rec, n);
   return 0;
 }
@@ -219,7 +220,7 @@ int main(void) {
           "ppcb_bunch": T.BUNCH_DTYPE.itemsize, "ppcb_run_info": C.sizeof(_lib.RunInfo),
           "ppcb_info": C.sizeof(_lib.Info), "ppcb_batch_info": C.sizeof(_lib.BatchInfo),
           "ppcb_tune_info": C.sizeof(_lib.TuneInfo), "ppcb_grad_info": C.sizeof(_lib.GradInfo),
-          "ppcb_ctrl": C.sizeof(T.Ctrl), "ppcb_params": C.sizeof(T.Params)}
+          "ppcb_ctrl": C.sizeof(T.Ctrl), "ppcb_params": C.sizeof(T.Params), "ppcb_acc_hit": T.ACC_DTYPE.itemsize}
     for k, v in py.items():
         assert int(c[k]) == v, (k, c[k], v)
     d = _lib.HITZ_DTYPE

@@ -92,3 +92,77 @@ def test_program_linked_against_libxppc_runs(ice_full, tmp_path):
     assert r.returncode == 0, (r.stdout[-500:], r.stderr[-2000:])
     n = int([l for l in r.stdout.splitlines() if l.startswith("hitz")][0].split()[1])
     assert n > 100
+
+
+def test_device_back_end_matches_host_back_end(ice_full2d, monkeypatch):
+    """ppcb_accept (the back end on the GPU) against eout()'s host back end on the same
+    kernel-level hits, on a detector with tilted sensor axes and cable azimuths: the two draw
+    different random numbers, so the accepted fraction, the per-DOM counts and the
+    wavelength and time distributions agree statistically, and a hit both accept carries
+    the same impact point and direction."""
+    from scipy import stats
+    monkeypatch.setenv("FLDR", "3960")
+    monkeypatch.setenv("ELEV", "30")
+    c = PPC()
+    c.initialize(1.0, ice_full2d)
+    c.set_seed(5)
+    c.choose(0)
+    c.ini()
+    c.keep_raw(True)
+    raws, hosts = [], []
+    for e, (s, om) in enumerate([(40, 30), (21, 20), (60, 40), (5, 50)]):
+        c.flset(s, om)
+        c.sett(0.0, 0.0, 1.0, (e, 7), 0)
+        c.flone(600_000_000)
+        c.eout()
+        hosts.append(c.hitz())
+        raws.append(c.raw_hits())
+        c.efin()
+    raw = np.concatenate(raws)
+    host = np.concatenate(hosts)
+    dev = c.accept(raw, seed=11)
+    c.close()
+    n = len(raw)
+    assert n > 50000 and len(host) > 5000, (n, len(host))
+    assert np.all(np.diff(dev["hit"].astype(np.int64)) > 0)  # input order
+    p_host, p_dev = len(host) / n, len(dev) / n
+    sd = np.sqrt(2 * p_host * (1 - p_host) / n)
+    assert abs(p_host - p_dev) < 4 * sd, (p_host, p_dev, sd)
+    # per-DOM counts (two-sample chi-square over DOMs with enough hits)
+    key_h = host["str"].astype(np.int64) * 100 + host["om"]
+    key_d = dev["str"].astype(np.int64) * 100 + dev["om"]
+    doms = np.union1d(key_h, key_d)
+    ch = np.array([np.count_nonzero(key_h == k) for k in doms])
+    cd = np.array([np.count_nonzero(key_d == k) for k in doms])
+    m = ch + cd >= 30
+    assert m.sum() >= 10
+    p_chi = stats.chi2_contingency(np.vstack([ch[m], cd[m]]))[1]
+    assert p_chi > 1e-3, p_chi
+    assert stats.ks_2samp(host["n"][:, 3], dev["wv"]).pvalue > 0.01
+    assert stats.ks_2samp(host["r"][:, 3], dev["t"]).pvalue > 0.01
+    # hits both back ends accepted: same geometry.  A host record is traced to its
+    # kernel-level hit by (event, arrival time); times two hits share are left out.
+    index = {}
+    base = 0
+    for e, r in enumerate(raws):
+        for j, t in enumerate(r["t"]):
+            key = (e + 1, float(t))
+            index[key] = -1 if key in index else base + j
+        base += len(r)
+    at = {int(k): j for j, k in enumerate(dev["hit"])}
+    both = ambiguous = 0
+    for h in host:
+        k = index.get((int(h["track_first"]) + 1, float(h["r"][3])))
+        assert k is not None
+        if k < 0:
+            ambiguous += 1
+            continue
+        j = at.get(k)
+        if j is None:
+            continue
+        both += 1
+        d = dev[j]
+        assert d["str"] == h["str"] and d["om"] == h["om"]
+        assert np.allclose(d["r"], h["r"][:3], atol=2e-5) and np.allclose(d["d"], h["n"][:3], atol=2e-5)
+    assert ambiguous < 0.05 * len(host)
+    assert both > 0.5 * min(len(host), len(dev)) * p_dev, (both, len(host), len(dev), p_dev)
