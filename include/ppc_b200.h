@@ -174,6 +174,7 @@ typedef struct ppcb_tune_info {
 } ppcb_tune_info;
 int ppcb_batch_create(ppcb_ctx* c, int device, uint32_t max_events, uint32_t max_bunches, uint64_t hit_capacity,
                       ppcb_batch** out);
+/* every ppcb_batch is destroyed before the ppcb_ctx it was created with */
 int ppcb_batch_destroy(ppcb_batch* b);
 int ppcb_batch_set_graph(ppcb_batch* b, int use_graph);
 int ppcb_batch_run(ppcb_batch* b, const ppcb_bunch* bunches, int32_t nb, uint32_t events, double hits_per_photon,
@@ -244,6 +245,81 @@ int ppcb_accept_device(ppcb_ctx* c, int device, const ppcb_hit* hits, uint64_t n
                        unsigned long long* count, void* stream);
 int ppcb_accept(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n, uint32_t seed, ppcb_acc_hit* out, uint64_t cap,
                 uint64_t* nout);
+
+/* ---- DirectFit likelihood on the device ----
+ * The saturated Poisson likelihood with model error that DirectFit fits with
+ * (llh/llh.cxx:419-662, 1075-1082), with the simulation side on the GPU.  ppcb_llh_create
+ * prepares the observed side once per event on the host, as dat::prep/optimize do:
+ *   - observed hits binned per DOM in 200 bins of lbin ns from the earliest hit;
+ *   - DOMs selected by total charge (qmin < q/drep < qsat) and flasher distance;
+ *   - each DOM's bins outside its window around the peak (500 ns before, 1000 ns after)
+ *     dropped;
+ *   - the remaining bins merged into blocks by the Bayesian-blocks partition of the
+ *     observed charge.
+ * ppcb_llh_eval_device then takes kernel-level hits and, in one pass over them, applies the
+ * back end's acceptance (the same per-hit streams as ppcb_accept with the same seed).  It
+ * bins the accepted hits of every DOM into its blocks for each of ndt time shifts and sums
+ * llf(simulated, observed, nsim, drep) over all blocks:
+ *   out[j] = (llf(nohit, 0, nsim, drep) [unless norm] + sum_DOM sum_block llf(...)) / ndof,
+ * as fllh(dts[j], nsim) does.  Hit times are on the observed hits' clock; a shift dt moves
+ * every simulated hit by +dt.  Simulated hits count 1 each (DirectFit without SPE charge
+ * sampling).  As in the reference, with norm a DOM that enters with all of its observed
+ * charge outside the 200 bins (dtot = 0) makes the result NaN.
+ * Not supported: the "good DOM" list, multi-PMT keys, the charge-unfolding variants. */
+typedef struct ppcb_llh ppcb_llh;
+typedef struct ppcb_llh_hit {        /* one observed pulse: the columns of DirectFit's dat file */
+  int32_t str, om;
+  double t, q;
+} ppcb_llh_hit;
+typedef struct ppcb_llh_window {     /* pulses of (str, om) with ti <= t < tf are ignored (ert) */
+  int32_t str, om;
+  double ti, tf;
+} ppcb_llh_window;
+typedef struct ppcb_llh_opts {
+  double lbin;    /* time bin [ns]; <= 0: max(25, (tmax - tmin + 1) / 200) (llh/llh.cxx:799) */
+  double sig;     /* model error of the saturated likelihood (LSSL::SIG, 0.10); 0: plain Poisson */
+  double qmin;    /* a DOM enters when qmin * drep < its charge < qsat * drep (0.1, 500) */
+  double qsat;
+  double drep;    /* repetitions of the observed data (1) */
+  int32_t peak;   /* window from the monotone-blocks fit instead of the highest bin (0) */
+  int32_t mono;   /* blocks rise to the peak and fall after it (0) */
+  int32_t norm;   /* normalise each DOM's simulation to its observed charge (0) */
+  int32_t unh;    /* count simulated hits on DOMs without data ("no-hit" term); DirectFit sets
+                     it when it reads a bad-DOM list (0) */
+  int32_t flasher, fla_str, fla_om, fsep; /* flasher run: leave out DOMs within fsep of it */
+} ppcb_llh_opts;
+typedef struct ppcb_llh_info {
+  double lbin, t0;  /* bin width and the time of bin 0 (earliest observed pulse) */
+  int32_t ndof;     /* 1 + blocks of the DOMs that enter */
+  int32_t doms;     /* DOMs that enter */
+  int32_t blocks;
+  int32_t errors;   /* llf evaluations whose Newton iteration left the domain (the reference
+                       stops there; here the term is NaN), summed since creation */
+} ppcb_llh_info;
+typedef struct ppcb_llh_block {      /* one block of one DOM: bins [first, last] and its charge */
+  int32_t str, om, first, last;
+  double dat;
+} ppcb_llh_block;
+#define PPCB_LLH_MAX_SHIFTS 64
+/* DirectFit's defaults (llh/llh.cxx:27-55, lssl.cxx:4) */
+int ppcb_llh_default_opts(ppcb_llh_opts* o);
+/* observed pulses (host), excluded windows and bad DOMs (str, om pairs; both may be null);
+ * device: the device of the ppcb_ctx whose acceptance and hits are used */
+int ppcb_llh_create(ppcb_ctx* c, int device, const ppcb_llh_hit* data, uint64_t n, const ppcb_llh_window* windows,
+                    uint64_t nwin, const int32_t* bad, uint64_t nbad, const ppcb_llh_opts* opts, ppcb_llh** out);
+/* every ppcb_llh is destroyed before the ppcb_ctx it was created with */
+int ppcb_llh_destroy(ppcb_llh* l);
+int ppcb_llh_get_info(ppcb_llh* l, ppcb_llh_info* info);
+/* blocks in DOM order, each DOM's from its last bin backwards (the order llh() sums them) */
+int ppcb_llh_blocks(ppcb_llh* l, ppcb_llh_block* out, uint64_t cap, uint64_t* n);
+/* hits: kernel-level hits in device memory; dts (host, ndt <= PPCB_LLH_MAX_SHIFTS); out: ndt
+ * doubles in device memory, written on `stream` */
+int ppcb_llh_eval_device(ppcb_llh* l, const ppcb_hit* hits, uint64_t n, uint32_t seed, const double* dts, int32_t ndt,
+                         double nsim, double* out, void* stream);
+/* the same with host buffers (copies included); fails with status 1 when an llf evaluation
+ * left its domain, as the reference exits */
+int ppcb_llh_eval(ppcb_llh* l, const ppcb_hit* hits, uint64_t n, uint32_t seed, const double* dts, int32_t ndt,
+                  double nsim, double* out);
 
 /* ---- measurement ----
  * No counterpart in the reference.  FP32 FMA throughput of `device` (TFLOP/s, best of

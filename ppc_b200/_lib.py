@@ -46,6 +46,18 @@ class GradInfo(C.Structure):
                 ("backward_ms", C.c_double)]
 
 
+class LlhOpts(C.Structure):
+    _fields_ = [("lbin", C.c_double), ("sig", C.c_double), ("qmin", C.c_double), ("qsat", C.c_double),
+                ("drep", C.c_double), ("peak", C.c_int32), ("mono", C.c_int32), ("norm", C.c_int32),
+                ("unh", C.c_int32), ("flasher", C.c_int32), ("fla_str", C.c_int32), ("fla_om", C.c_int32),
+                ("fsep", C.c_int32)]
+
+
+class LlhInfo(C.Structure):
+    _fields_ = [("lbin", C.c_double), ("t0", C.c_double), ("ndof", C.c_int32), ("doms", C.c_int32),
+                ("blocks", C.c_int32), ("errors", C.c_int32)]
+
+
 class Dom(C.Structure):
     _fields_ = [("R", C.c_float), ("F", C.c_float), ("r", C.c_float * 3)]
 
@@ -66,7 +78,8 @@ EXPORTS = [
     "ppcb_rng_reset", "ppcb_table", "ppcb_generate_device", "ppcb_index_probe_device", "ppcb_propagate_noalloc",
     "ppcb_batch_create", "ppcb_batch_destroy", "ppcb_batch_set_graph", "ppcb_batch_run", "ppcb_batch_counts",
     "ppcb_batch_hits", "ppcb_batch_autotune", "ppcb_set_ice", "ppcb_get_ice", "ppcb_gradient",
-    "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept",
+    "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept", "ppcb_llh_default_opts", "ppcb_llh_create",
+    "ppcb_llh_destroy", "ppcb_llh_get_info", "ppcb_llh_blocks", "ppcb_llh_eval_device", "ppcb_llh_eval",
 ]
 
 
@@ -130,6 +143,13 @@ def lib():
         "ppcb_fp32_peak": (i32, [i32, i32, P(f64), P(f64)]),
         "ppcb_accept_device": (i32, [vp, i32, vp, u64, u32, vp, vp, vp]),
         "ppcb_accept": (i32, [vp, vp, u64, u32, vp, u64, P(u64)]),
+        "ppcb_llh_default_opts": (i32, [P(LlhOpts)]),
+        "ppcb_llh_create": (i32, [vp, i32, vp, u64, vp, u64, vp, u64, P(LlhOpts), P(vp)]),
+        "ppcb_llh_destroy": (i32, [vp]),
+        "ppcb_llh_get_info": (i32, [vp, P(LlhInfo)]),
+        "ppcb_llh_blocks": (i32, [vp, vp, u64, P(u64)]),
+        "ppcb_llh_eval_device": (i32, [vp, vp, u64, u32, vp, i32, f64, vp, vp]),
+        "ppcb_llh_eval": (i32, [vp, vp, u64, u32, vp, i32, f64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

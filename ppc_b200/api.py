@@ -13,6 +13,7 @@
 Errors raise PPCError with the reference's exit status as `.code`.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -27,6 +28,7 @@ def _p(a):
 class PPC:
     def __init__(self):
         self._c = C.c_void_p()
+        self._children = weakref.WeakSet()  # handles made from this context, closed before it
         check(lib().ppcb_create(C.byref(self._c)))
 
     # ---- lifecycle -------------------------------------------------------------
@@ -53,6 +55,8 @@ class PPC:
         check(lib().ppcb_fin(self._c))
 
     def close(self):
+        for h in list(getattr(self, "_children", ())):
+            h.close()
         if self._c:
             lib().ppcb_destroy(self._c)
             self._c = C.c_void_p()
@@ -220,6 +224,7 @@ class Batch:
         check(lib().ppcb_batch_create(ctx._c, device, int(max_events), int(max_bunches), int(hit_capacity),
                                       C.byref(self._b)))
         self.events = 0
+        ctx._children.add(self)
 
     def set_graph(self, use):
         check(lib().ppcb_batch_set_graph(self._b, int(bool(use))))
@@ -335,3 +340,74 @@ def _accept(self, hits, seed=0):
 
 
 PPC.accept = _accept
+
+
+class Likelihood:
+    """DirectFit's likelihood (llh/llh.cxx:419-662, 1075-1082) with the simulation side on
+    the GPU (ppcb_llh_*).  `data`: observed pulses (LLH_HIT_DTYPE: str, om, t, q), prepared
+    once on the host: binned per DOM, DOMs selected, each DOM's bins merged into blocks.
+    `eval(hits, dts, nsim, seed)` takes kernel-level hits, applies the back end's
+    acceptance (as PPC.accept with the same seed) and returns fllh(dt, nsim) for every
+    shift dt.  Options (DirectFit's names and defaults): lbin (0: automatic), sig (0.10),
+    qmin (0.1), qsat (500), drep (1), peak, mono, norm, unh (0), flasher, fla_str,
+    fla_om (0), fsep (1)."""
+
+    def __init__(self, ctx, data, windows=None, bad=None, device=0, **opts):
+        from ._lib import LlhOpts
+        o = LlhOpts()
+        check(lib().ppcb_llh_default_opts(C.byref(o)))
+        for k, v in opts.items():
+            if k not in dict(LlhOpts._fields_):
+                raise TypeError(f"unknown likelihood option {k!r}")
+            setattr(o, k, v)
+        data = np.ascontiguousarray(data, T.LLH_HIT_DTYPE)
+        win = np.ascontiguousarray(windows if windows is not None else np.zeros(0, T.LLH_WINDOW_DTYPE),
+                                   T.LLH_WINDOW_DTYPE)
+        badk = np.ascontiguousarray(bad if bad is not None else np.zeros((0, 2)), np.int32).reshape(-1, 2)
+        self._ctx = ctx  # keeps the context alive
+        self._h = C.c_void_p()
+        check(lib().ppcb_llh_create(ctx._c, int(device), _p(data), len(data), _p(win) if len(win) else None,
+                                    len(win), _p(badk) if len(badk) else None, len(badk), C.byref(o),
+                                    C.byref(self._h)))
+        self.opts = {k: getattr(o, k) for k, _ in LlhOpts._fields_}
+        ctx._children.add(self)
+
+    def info(self):
+        from ._lib import LlhInfo
+        i = LlhInfo()
+        check(lib().ppcb_llh_get_info(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in LlhInfo._fields_}
+
+    def blocks(self):
+        n = C.c_uint64()
+        check(lib().ppcb_llh_blocks(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(1, n.value), T.LLH_BLOCK_DTYPE)
+        check(lib().ppcb_llh_blocks(self._h, _p(out), len(out), C.byref(n)))
+        return out[:n.value]
+
+    def eval(self, hits, dts=(0.0,), nsim=1.0, seed=0):
+        hits = np.ascontiguousarray(hits, T.HIT_DTYPE)
+        dts = np.ascontiguousarray(np.atleast_1d(dts), np.float64)
+        out = np.zeros(len(dts), np.float64)
+        check(lib().ppcb_llh_eval(self._h, _p(hits) if len(hits) else None, len(hits), int(seed) & 0xFFFFFFFF,
+                                  _p(dts), len(dts), float(nsim), _p(out)))
+        return out
+
+    def eval_device(self, hits_ptr, n, dts, nsim, out_ptr, seed=0, stream=0):
+        """Asynchronous evaluation over device memory (raw pointers: n kernel-level hits,
+        len(dts) doubles out)."""
+        dts = np.ascontiguousarray(np.atleast_1d(dts), np.float64)
+        check(lib().ppcb_llh_eval_device(self._h, C.c_void_p(hits_ptr), int(n), int(seed) & 0xFFFFFFFF, _p(dts),
+                                         len(dts), float(nsim), C.c_void_p(out_ptr),
+                                         C.c_void_p(stream) if stream else None))
+
+    def close(self):
+        if self._h:
+            lib().ppcb_llh_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -33,10 +33,13 @@ NVFLAGS = ARCH + ["-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-Xcompil
 CXXFLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-result",
             "-I" + os.path.join(CUDA_HOME, "include"), "-I" + INC]
 
-CU = ["propagate.cu", "engine.cu", "noalloc.cu", "batch.cu", "gradient.cu", "peak.cu", "backend.cu"]
-CPP = ["config.cpp", "session.cpp", "capi.cpp", "capi_batch.cpp", "xppc.cpp"]
+CU = ["propagate.cu", "engine.cu", "noalloc.cu", "batch.cu", "gradient.cu", "peak.cu", "backend.cu", "llh.cu"]
+CPP = ["config.cpp", "session.cpp", "capi.cpp", "capi_batch.cpp", "capi_llh.cpp", "xppc.cpp", "llh.cpp"]
+# the likelihood's FP64 sums are kept free of fused multiply-adds, like the host code
+CU_EXTRA = {"llh.cu": ["--fmad=false"]}
 CLI = ["ppc_cli.cpp"]
-HEADERS = ["ppcb_types.h", "config.h", "engine.h", "propagate.cuh", "session.h", "ctx.h", "tilt.h", "batch.h"]
+HEADERS = ["ppcb_types.h", "config.h", "engine.h", "propagate.cuh", "session.h", "ctx.h", "tilt.h", "batch.h",
+           "backend.cuh", "llh.h"]
 
 
 def _newer(target, deps):
@@ -66,7 +69,8 @@ def build(verbose=False):
     for f in CU:
         src, obj = os.path.join(SRC, f), os.path.join(OBJ, f + ".o")
         if _newer(obj, [src] + hdrs):
-            _run([NVCC] + NVFLAGS + ["-c", src, "-o", obj], log=os.path.join(OBJ, f + ".ptxas.txt"))
+            _run([NVCC] + NVFLAGS + CU_EXTRA.get(f, []) + ["-c", src, "-o", obj],
+                 log=os.path.join(OBJ, f + ".ptxas.txt"))
         objs.append(obj)
     for f in CPP:
         src, obj = os.path.join(SRC, f), os.path.join(OBJ, f + ".o")

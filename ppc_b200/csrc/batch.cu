@@ -63,7 +63,8 @@ Batch::Batch(Engine& e, int device, uint32_t max_events, uint32_t max_bunches, u
   if (!e.ready()) throw Error("ini() must come before creating a batch", 6);
   if (device < 0 || device >= (int)e.devs.size()) throw Error("bad device index", 7);
   if (max_events == 0 || max_bunches == 0) throw Error("empty batch capacity", 7);
-  check(cudaSetDevice(e.devs[d_].dev), "cudaSetDevice");
+  cuda_dev_ = e.devs[d_].dev;
+  check(cudaSetDevice(cuda_dev_), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "stream");
   for (cudaEvent_t* ev : {&k0_, &k1_, &g0_, &g1_}) check(cudaEventCreate(ev), "event");
   bunches_ = dmalloc<ppcb_bunch>(maxB_);
@@ -92,7 +93,7 @@ Batch::Batch(Engine& e, int device, uint32_t max_events, uint32_t max_bunches, u
 }
 
 Batch::~Batch() {
-  cudaSetDevice(eng_.devs[d_].dev);
+  cudaSetDevice(cuda_dev_);
   if (st_) cudaStreamSynchronize(st_);
   release_graph();
   void* d[] = {bunches_, bstart_, ev_off_, ev_cap_, ev_cnt_, dyn_, hits_, out_, out_off_, ctrl_};

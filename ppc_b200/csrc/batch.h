@@ -46,6 +46,7 @@ class Batch {
   void release_graph();
   Engine& eng_;
   int d_;
+  int cuda_dev_ = -1;  // the CUDA device of the buffers (frees them without the engine)
   uint32_t maxE_, maxB_;
   uint64_t hcap_;
   cudaStream_t st_ = nullptr;

@@ -126,12 +126,13 @@ class Engine {
   // (device pointer), on stream st.  Standard sensors only.
   void accept(int d, const ppcb_hit* dhits, uint64_t n, uint32_t seed, ppcb_acc_hit* dout,
               unsigned long long* dcount, cudaStream_t st);
+  // The back end's tables on device `d` (built from the configuration on first use).
+  BackendTables& backend_tables(int d);
   double total_device_ms() const;
   KArgs args_for(int d) const;
 
  private:
   void free_device(DeviceCtx& g);
-  void accept_tables(int d);
   std::shared_ptr<GradScratch> gs_;  // grows to the largest gradient call; freed by fin()
   bool inited_ = false;
   bool initialized_ = false;

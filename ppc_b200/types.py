@@ -56,6 +56,11 @@ HIT_DTYPE = np.dtype([("i", "<u4"), ("n", "<u4"), ("z", "<u4"), ("t", "<f4"),
 ACC_DTYPE = np.dtype([("i", "<u4"), ("n", "<u4"), ("hit", "<u4"), ("str", "<i4"), ("om", "<i4"), ("pmt", "<i4"),
                       ("t", "<f4"), ("wv", "<f4"), ("r", "<f4", 3), ("d", "<f4", 3)])
 
+# DirectFit likelihood records (ppcb_llh_hit / _window / _block), 24 bytes each
+LLH_HIT_DTYPE = np.dtype([("str", "<i4"), ("om", "<i4"), ("t", "<f8"), ("q", "<f8")])
+LLH_WINDOW_DTYPE = np.dtype([("str", "<i4"), ("om", "<i4"), ("ti", "<f8"), ("tf", "<f8")])
+LLH_BLOCK_DTYPE = np.dtype([("str", "<i4"), ("om", "<i4"), ("first", "<i4"), ("last", "<i4"), ("dat", "<f8")])
+
 # photon bunch, 64 bytes; the 16-byte union is exposed both ways
 BUNCH_DTYPE = np.dtype([("r", "<f4", 4), ("n", "<f4", 4), ("q", "<u4"), ("num", "<u4"),
                         ("type", "<i4"), ("f", "<f4"), ("u", "<u4", 4)])

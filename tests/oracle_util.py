@@ -208,3 +208,85 @@ def mwc_init(seed, rm):
     """Initial stream state of every thread: (362436069 + seed, 1234567), gpu/ini.cxx:556-571."""
     v = np.uint64((362436069 + seed) & 0xFFFFFFFF) | (np.uint64(1234567) << np.uint64(32))
     return np.full(len(rm), v, np.uint64)
+
+
+# ---- DirectFit likelihood oracle (oracle/libllh_oracle.so) ----------------------------------
+LLH_ORACLE_SO = os.path.join(ROOT, "oracle", "libllh_oracle.so")
+
+
+class LlhoOpts(C.Structure):
+    _fields_ = [("lbin", C.c_double), ("sig", C.c_double), ("qmin", C.c_double), ("qsat", C.c_double),
+                ("drep", C.c_double), ("peak", C.c_int32), ("mono", C.c_int32), ("norm", C.c_int32),
+                ("unh", C.c_int32), ("flasher", C.c_int32), ("fla_str", C.c_int32), ("fla_om", C.c_int32),
+                ("fsep", C.c_int32)]
+
+
+LLHO_DEFAULTS = dict(lbin=0.0, sig=0.10, qmin=0.1, qsat=500.0, drep=1.0, peak=0, mono=0, norm=0, unh=0, flasher=0,
+                     fla_str=0, fla_om=0, fsep=1)
+LLHO_SIM_DTYPE = np.dtype([("str", "<i4"), ("om", "<i4"), ("t", "<f4")])
+
+_llh = None
+
+
+def llh_lib():
+    global _llh
+    if _llh is None:
+        if not os.path.exists(LLH_ORACLE_SO):
+            raise RuntimeError("likelihood oracle missing: run `make -C oracle oracle`")
+        L = C.CDLL(LLH_ORACLE_SO)
+        vp, lg, i32, f64 = C.c_void_p, C.c_long, C.c_int, C.c_double
+        L.llho_llf.restype = f64
+        L.llho_llf.argtypes = [f64, f64, f64, f64, f64, C.POINTER(i32)]
+        L.llho_setup.restype = i32
+        L.llho_setup.argtypes = [vp, lg, vp, lg, vp, lg, vp, vp, lg, C.POINTER(lg), C.POINTER(f64), C.POINTER(f64),
+                                 C.POINTER(i32)]
+        L.llho_fllh.restype = i32
+        L.llho_fllh.argtypes = [vp, lg, vp, lg, vp, lg, vp, vp, lg, vp, i32, f64, vp, C.POINTER(i32)]
+        _llh = L
+    return _llh
+
+
+def llf(s, d, nsim, ndat, sig=0.10):
+    err = C.c_int(0)
+    v = llh_lib().llho_llf(float(s), float(d), float(nsim), float(ndat), float(sig), C.byref(err))
+    return v, err.value
+
+
+def _llh_inputs(data, windows, bad, opts):
+    o = LlhoOpts(**{**LLHO_DEFAULTS, **(opts or {})})
+    data = np.ascontiguousarray(data, T.LLH_HIT_DTYPE)
+    win = np.ascontiguousarray(windows if windows is not None else np.zeros(0, T.LLH_WINDOW_DTYPE),
+                               T.LLH_WINDOW_DTYPE)
+    badk = np.ascontiguousarray(bad if bad is not None else np.zeros((0, 2)), np.int32).reshape(-1, 2)
+    ptr = lambda a: C.c_void_p(a.ctypes.data) if len(a) else None
+    return o, data, win, badk, ptr
+
+
+def llh_setup(data, windows=None, bad=None, opts=None):
+    """The oracle's observed side: (blocks, lbin, t0, ndof), or None where it reports an error."""
+    o, data, win, badk, ptr = _llh_inputs(data, windows, bad, opts)
+    cap = 200 * (len(np.unique(data[["str", "om"]])) + len(win) + 1)
+    out = np.zeros(cap, T.LLH_BLOCK_DTYPE)
+    nb, lbin, t0, ndof = C.c_long(), C.c_double(), C.c_double(), C.c_int()
+    r = llh_lib().llho_setup(ptr(data), len(data), ptr(win), len(win), ptr(badk), len(badk), C.byref(o),
+                             C.c_void_p(out.ctypes.data), cap, C.byref(nb), C.byref(lbin), C.byref(t0),
+                             C.byref(ndof))
+    if r != 0:
+        return None
+    return out[:nb.value], lbin.value, t0.value, ndof.value
+
+
+def llh_fllh(data, sim, dts, nsim, windows=None, bad=None, opts=None):
+    """fllh(dt, nsim) for every dt over the accepted simulated hits `sim` (str, om, t)."""
+    o, data, win, badk, ptr = _llh_inputs(data, windows, bad, opts)
+    s = np.zeros(len(sim), LLHO_SIM_DTYPE)
+    if len(sim):
+        s["str"], s["om"], s["t"] = sim["str"], sim["om"], sim["t"]
+    dts = np.ascontiguousarray(np.atleast_1d(dts), np.float64)
+    out = np.zeros(len(dts))
+    err = C.c_int()
+    r = llh_lib().llho_fllh(ptr(data), len(data), ptr(win), len(win), ptr(badk), len(badk), C.byref(o), ptr(s),
+                            len(s), C.c_void_p(dts.ctypes.data), len(dts), float(nsim),
+                            C.c_void_p(out.ctypes.data), C.byref(err))
+    assert r == 0
+    return out, err.value

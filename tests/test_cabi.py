@@ -207,6 +207,11 @@ int main(void) {
   printf("ppcb_ctrl %zu\\n", sizeof(ppcb_ctrl));
   printf("ppcb_params %zu\\n", sizeof(ppcb_params));
   printf("ppcb_acc_hit %zu\\n", sizeof(ppcb_acc_hit));
+  printf("ppcb_llh_hit %zu\\n", sizeof(ppcb_llh_hit));
+  printf("ppcb_llh_window %zu\\n", sizeof(ppcb_llh_window));
+  printf("ppcb_llh_block %zu\\n", sizeof(ppcb_llh_block));
+  printf("ppcb_llh_opts %zu\\n", sizeof(ppcb_llh_opts));
+  printf("ppcb_llh_info %zu\\n", sizeof(ppcb_llh_info));
   F(ppcb_hitz_rec, t0); F(ppcb_hitz_rec, str); F(ppcb_hitz_rec, r); F(ppcb_hitz_rec, n);
   return 0;
 }
@@ -220,7 +225,10 @@ int main(void) {
           "ppcb_bunch": T.BUNCH_DTYPE.itemsize, "ppcb_run_info": C.sizeof(_lib.RunInfo),
           "ppcb_info": C.sizeof(_lib.Info), "ppcb_batch_info": C.sizeof(_lib.BatchInfo),
           "ppcb_tune_info": C.sizeof(_lib.TuneInfo), "ppcb_grad_info": C.sizeof(_lib.GradInfo),
-          "ppcb_ctrl": C.sizeof(T.Ctrl), "ppcb_params": C.sizeof(T.Params), "ppcb_acc_hit": T.ACC_DTYPE.itemsize}
+          "ppcb_ctrl": C.sizeof(T.Ctrl), "ppcb_params": C.sizeof(T.Params), "ppcb_acc_hit": T.ACC_DTYPE.itemsize,
+          "ppcb_llh_hit": T.LLH_HIT_DTYPE.itemsize, "ppcb_llh_window": T.LLH_WINDOW_DTYPE.itemsize,
+          "ppcb_llh_block": T.LLH_BLOCK_DTYPE.itemsize, "ppcb_llh_opts": C.sizeof(_lib.LlhOpts),
+          "ppcb_llh_info": C.sizeof(_lib.LlhInfo)}
     for k, v in py.items():
         assert int(c[k]) == v, (k, c[k], v)
     d = _lib.HITZ_DTYPE
