@@ -246,6 +246,33 @@ int ppcb_accept_device(ppcb_ctx* c, int device, const ppcb_hit* hits, uint64_t n
 int ppcb_accept(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n, uint32_t seed, ppcb_acc_hit* out, uint64_t cap,
                 uint64_t* nout);
 
+/* ---- source front end on the device ----
+ * The library's sources (addp with particle types, addp_clst, addp_mopo; f2k "ph" records)
+ * become photon bunches on the GPU, as the host front end makes them (gpu/f2k.cxx:17-167,
+ * 377-528):
+ *   - light yield per particle type: muon segments, EM cascades, hadronic cascades with
+ *     their charge fluctuation;
+ *   - times the efficiency, over the DOM oversize factor;
+ *   - a Poisson-sampled photon count (exact counts for clst and "ph").
+ * A source makes one bunch, or several of at most 2^31 photons each.  Each source draws
+ * from its own random stream keyed by (seed, source index), so the counts match the host
+ * front end in distribution, not source for source.  The bunches feed
+ * ppcb_propagate_device directly: bstart[k] is the first photon of bunch k and bstart[nb]
+ * the total. */
+/* src: device pointer, ns sources; out: room for cap bunches; bstart: cap + 1 entries;
+ * counts (device, 2 x uint64): bunches needed and photons.  When counts[0] > cap only the
+ * first cap bunches are written (call again with more room).  Asynchronous on `stream`. */
+int ppcb_sources_device(ppcb_ctx* c, int device, const ppcb_source* src, uint64_t ns, uint32_t seed,
+                        ppcb_bunch* out, uint64_t* bstart, uint64_t cap, uint64_t* counts, void* stream);
+/* host buffers, device 0; *nb and *num receive the bunches needed and the photons */
+int ppcb_sources(ppcb_ctx* c, const ppcb_source* src, uint64_t ns, uint32_t seed, ppcb_bunch* out, uint64_t* bstart,
+                 uint64_t cap, uint64_t* nb, uint64_t* num);
+/* f2k text (TR records, one segment per line, gpu/f2k.cxx:555-583) to sources; the first
+ * line is segment first_segment.  *n receives the number of sources, at most cap written;
+ * *lines the number of lines (segments) read. */
+int ppcb_f2k_sources(const char* text, uint64_t len, uint32_t first_segment, ppcb_source* out, uint64_t cap,
+                     uint64_t* n, uint64_t* lines);
+
 /* ---- DirectFit likelihood on the device ----
  * The saturated Poisson likelihood with model error that DirectFit fits with
  * (llh/llh.cxx:419-662, 1075-1082), with the simulation side on the GPU.  ppcb_llh_create

@@ -16,6 +16,10 @@
 // usage:
 //   ref_harness tables <out.bin>
 //   ref_harness zshift <in.f32x4> <out.f32x3>
+//   ref_harness yield <in> <out>
+//      in: (f32 E, f32 dr, i32 type, f32 scale) per source; out: (f32 mean, f32 f, f32 a,
+//      f32 b, f32 length, f32 yield) per source -- the bunch template addp() makes and the
+//      Poisson mean it samples (gpu/f2k.cxx:17-167, 484-504)
 //   ref_harness run <spec> <photons> <seed> <out-prefix> [nodump]
 //      spec = "flasher:<str>:<om>" | "cascade:<x>:<y>:<z>:<E>:<nx>:<ny>:<nz>:<type>"
 //           | "point:<x>:<y>:<z>"   (isotropic point source, FWID=-1 style, at x,y,z)
@@ -131,6 +135,24 @@ int main(int argc, char** argv) {
   if (mode == "zshift" && argc >= 4) {
     initialize();
     do_zshift(argv[2], argv[3]);
+    return 0;
+  }
+  if (mode == "yield" && argc >= 4) {
+    initialize();
+    FILE* f = xopen(argv[2], "rb");
+    std::vector<float> out;
+    struct { float E, dr; int type; float scale; } src;
+    while (fread(&src, sizeof(src), 1, f) == 1) {
+      p = photon();
+      const float y = yield(src.E, src.dr, src.type);
+      const float mean = src.scale * y / ovr;
+      const float rec[6] = {mean, p.f, p.a, p.b, p.n.w, y};
+      out.insert(out.end(), rec, rec + 6);
+    }
+    fclose(f);
+    f = xopen(argv[3], "wb");
+    fwrite(out.data(), sizeof(float), out.size(), f);
+    fclose(f);
     return 0;
   }
   if (mode == "run" && argc >= 6) {

@@ -80,6 +80,7 @@ EXPORTS = [
     "ppcb_batch_hits", "ppcb_batch_autotune", "ppcb_set_ice", "ppcb_get_ice", "ppcb_gradient",
     "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept", "ppcb_llh_default_opts", "ppcb_llh_create",
     "ppcb_llh_destroy", "ppcb_llh_get_info", "ppcb_llh_blocks", "ppcb_llh_eval_device", "ppcb_llh_eval",
+    "ppcb_sources_device", "ppcb_sources", "ppcb_f2k_sources",
 ]
 
 
@@ -143,6 +144,9 @@ def lib():
         "ppcb_fp32_peak": (i32, [i32, i32, P(f64), P(f64)]),
         "ppcb_accept_device": (i32, [vp, i32, vp, u64, u32, vp, vp, vp]),
         "ppcb_accept": (i32, [vp, vp, u64, u32, vp, u64, P(u64)]),
+        "ppcb_sources_device": (i32, [vp, i32, vp, u64, u32, vp, vp, u64, vp, vp]),
+        "ppcb_sources": (i32, [vp, vp, u64, u32, vp, vp, u64, P(u64), P(u64)]),
+        "ppcb_f2k_sources": (i32, [C.c_char_p, u64, u32, vp, u64, P(u64), P(u64)]),
         "ppcb_llh_default_opts": (i32, [P(LlhOpts)]),
         "ppcb_llh_create": (i32, [vp, i32, vp, u64, vp, u64, vp, u64, P(LlhOpts), P(vp)]),
         "ppcb_llh_destroy": (i32, [vp]),

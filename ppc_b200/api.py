@@ -342,6 +342,37 @@ def _accept(self, hits, seed=0):
 PPC.accept = _accept
 
 
+def _sources(self, src, seed=0, cap=None):
+    """Device front end (ppcb_sources): sources (SOURCE_DTYPE) to photon bunches, Poisson
+    counts drawn on the GPU.  Returns (bunches, bstart, photons); bstart[k] is the first
+    photon of bunch k, bstart[-1] the total, ready for propagate_device."""
+    src = np.ascontiguousarray(src, T.SOURCE_DTYPE)
+    cap = len(src) + 8 if cap is None else int(cap)
+    while True:
+        out = np.zeros(max(1, cap), T.BUNCH_DTYPE)
+        bstart = np.zeros(cap + 1, np.uint64)
+        nb, num = C.c_uint64(), C.c_uint64()
+        check(lib().ppcb_sources(self._c, _p(src) if len(src) else None, len(src), int(seed) & 0xFFFFFFFF, _p(out),
+                                 _p(bstart), cap, C.byref(nb), C.byref(num)))
+        if nb.value <= cap:
+            return out[:nb.value], bstart[:nb.value + 1], num.value
+        cap = nb.value
+
+
+PPC.sources = _sources
+
+
+def f2k_sources(text, first_segment=1):
+    """f2k text (TR records, one segment per line) to SOURCE_DTYPE records for the device
+    front end; returns (sources, lines read)."""
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    n, lines = C.c_uint64(), C.c_uint64()
+    check(lib().ppcb_f2k_sources(b, len(b), int(first_segment), None, 0, C.byref(n), C.byref(lines)))
+    out = np.zeros(max(1, n.value), T.SOURCE_DTYPE)
+    check(lib().ppcb_f2k_sources(b, len(b), int(first_segment), _p(out), len(out), C.byref(n), C.byref(lines)))
+    return out[:n.value], lines.value
+
+
 class Likelihood:
     """DirectFit's likelihood (llh/llh.cxx:419-662, 1075-1082) with the simulation side on
     the GPU (ppcb_llh_*).  `data`: observed pulses (LLH_HIT_DTYPE: str, om, t, q), prepared

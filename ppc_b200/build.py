@@ -28,15 +28,19 @@ CXX = os.environ.get("PPCB_CXX", "/usr/bin/g++" if os.path.exists("/usr/bin/g++"
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ARCH + ["-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                  "-Xptxas", "-v", "-I" + INC]
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-I" + INC]
 CXXFLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-result",
             "-I" + os.path.join(CUDA_HOME, "include"), "-I" + INC]
 
-CU = ["propagate.cu", "engine.cu", "noalloc.cu", "batch.cu", "gradient.cu", "peak.cu", "backend.cu", "llh.cu"]
+CU = ["propagate.cu", "engine.cu", "noalloc.cu", "batch.cu", "gradient.cu", "peak.cu", "backend.cu", "llh.cu",
+      "frontend.cu"]
 CPP = ["config.cpp", "session.cpp", "capi.cpp", "capi_batch.cpp", "capi_llh.cpp", "xppc.cpp", "llh.cpp"]
-# the likelihood's FP64 sums are kept free of fused multiply-adds, like the host code
-CU_EXTRA = {"llh.cu": ["--fmad=false"]}
+# Fast math everywhere but in the front end, whose bunch templates follow the host front
+# end's float arithmetic (no approximate logf/powf, no contraction).  The likelihood
+# (llh.cu) repeats the back end's acceptance decisions, so it keeps the back end's flags.
+CU_EXTRA = {"frontend.cu": ["--fmad=false"]}
+CU_FAST_MATH = ["--use_fast_math"]
+CU_EXACT = {"frontend.cu"}
 CLI = ["ppc_cli.cpp"]
 HEADERS = ["ppcb_types.h", "config.h", "engine.h", "propagate.cuh", "session.h", "ctx.h", "tilt.h", "batch.h",
            "backend.cuh", "llh.h"]
@@ -69,7 +73,8 @@ def build(verbose=False):
     for f in CU:
         src, obj = os.path.join(SRC, f), os.path.join(OBJ, f + ".o")
         if _newer(obj, [src] + hdrs):
-            _run([NVCC] + NVFLAGS + CU_EXTRA.get(f, []) + ["-c", src, "-o", obj],
+            fast = [] if f in CU_EXACT else CU_FAST_MATH
+            _run([NVCC] + NVFLAGS + fast + CU_EXTRA.get(f, []) + ["-c", src, "-o", obj],
                  log=os.path.join(OBJ, f + ".ptxas.txt"))
         objs.append(obj)
     for f in CPP:

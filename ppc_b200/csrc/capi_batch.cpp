@@ -1,4 +1,5 @@
 // C ABI of the batched launch (declarations: include/ppc_b200.h, "batched events").
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -6,6 +7,7 @@
 #include "../../include/ppc_b200.h"
 #include "batch.h"
 #include "ctx.h"
+#include "session.h"
 
 struct ppcb_batch {
   ppcb::Batch* b = nullptr;
@@ -191,6 +193,110 @@ int ppcb_accept(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n, uint32_t seed, pp
       throw;
     }
     release();
+  });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int ppcb_sources_device(ppcb_ctx* c, int device, const ppcb_source* src, uint64_t ns, uint32_t seed,
+                        ppcb_bunch* out, uint64_t* bstart, uint64_t cap, uint64_t* counts, void* stream) {
+  if (!c || (ns > 0 && !src) || (cap > 0 && !out) || !bstart || !counts) {
+    ppcb_internal_set_error("null argument");
+    return PPCB_EARG;
+  }
+  return bguard([&] {
+    if (device < 0 || device >= (int)c->s.eng.devs.size()) throw ppcb::Error("bad device index", PPCB_EARG);
+    c->s.eng.sources(device, src, ns, seed, out, bstart, cap, counts, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int ppcb_sources(ppcb_ctx* c, const ppcb_source* src, uint64_t ns, uint32_t seed, ppcb_bunch* out, uint64_t* bstart,
+                 uint64_t cap, uint64_t* nb, uint64_t* num) {
+  if (!c || (ns > 0 && !src) || (cap > 0 && (!out || !bstart)) || !nb || !num) {
+    ppcb_internal_set_error("null argument");
+    return PPCB_EARG;
+  }
+  return bguard([&] {
+    ppcb::Engine& e = c->s.eng;
+    if (!e.ready()) throw ppcb::Error("ppcb_ini() must come before the front end", PPCB_ESTATE);
+    ppcb::check(cudaSetDevice(e.devs[0].dev), "cudaSetDevice");
+    const int before = e.front_errors(0);
+    ppcb_source* ds = nullptr;
+    ppcb_bunch* dout = nullptr;
+    uint64_t* dbs = nullptr;
+    uint64_t* dcnt = nullptr;
+    auto release = [&]() {
+      for (void* p : {(void*)ds, (void*)dout, (void*)dbs, (void*)dcnt})
+        if (p) cudaFree(p);
+    };
+    try {
+      ppcb::check(cudaMalloc((void**)&ds, std::max<uint64_t>(ns, 1) * sizeof(ppcb_source)), "front end input");
+      ppcb::check(cudaMalloc((void**)&dout, std::max<uint64_t>(cap, 1) * sizeof(ppcb_bunch)), "front end output");
+      ppcb::check(cudaMalloc((void**)&dbs, (cap + 1) * sizeof(uint64_t)), "front end output");
+      ppcb::check(cudaMalloc((void**)&dcnt, 2 * sizeof(uint64_t)), "front end counts");
+      if (ns) ppcb::check(cudaMemcpy(ds, src, ns * sizeof(ppcb_source), cudaMemcpyHostToDevice), "H2D sources");
+      e.sources(0, ds, ns, seed, dout, dbs, cap, dcnt, 0);
+      uint64_t cnt[2];
+      ppcb::check(cudaMemcpy(cnt, dcnt, sizeof(cnt), cudaMemcpyDeviceToHost), "D2H counts");
+      const uint64_t w = std::min<uint64_t>(cnt[0], cap);
+      if (w) ppcb::check(cudaMemcpy(out, dout, w * sizeof(ppcb_bunch), cudaMemcpyDeviceToHost), "D2H bunches");
+      if (cap > 0 || cnt[0] == 0)
+        if (bstart)
+          ppcb::check(cudaMemcpy(bstart, dbs, (w + (cnt[0] <= cap ? 1 : 0)) * sizeof(uint64_t),
+                                 cudaMemcpyDeviceToHost), "D2H bunch starts");
+      *nb = cnt[0];
+      *num = cnt[1];
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+    if (e.front_errors(0) != before)
+      throw ppcb::Error("front end: a source's sampling failed (negative type, bad count or no convergence)",
+                        PPCB_EARG);
+  });
+}
+
+int ppcb_f2k_sources(const char* text, uint64_t len, uint32_t first_segment, ppcb_source* out, uint64_t cap,
+                     uint64_t* n, uint64_t* lines) {
+  if ((len > 0 && !text) || (cap > 0 && !out) || !n || !lines) {
+    ppcb_internal_set_error("null argument");
+    return PPCB_EARG;
+  }
+  return bguard([&] {
+    uint64_t k = 0, line = 0, pos = 0;
+    while (pos < len) {
+      uint64_t end = pos;
+      while (end < len && text[end] != '\n') end++;
+      const std::string in(text + pos, end - pos);
+      pos = end + 1;
+      const uint32_t seg = first_segment + (uint32_t)line++;
+      ppcb::F2kTrack tr;
+      if (!ppcb::parse_f2k_track(in, tr) || tr.type == -1) continue;
+      if (k < cap) {
+        ppcb_source s;
+        std::memset(&s, 0, sizeof(s));
+        s.r[0] = tr.x; s.r[1] = tr.y; s.r[2] = tr.z; s.r[3] = tr.t;
+        s.n[0] = tr.n[0]; s.n[1] = tr.n[1]; s.n[2] = tr.n[2];
+        s.q = seg;
+        if (tr.type == -2) {
+          s.kind = PPCB_SRC_POINT;
+          s.amount = (double)(unsigned long long)tr.E;
+        } else {
+          s.kind = PPCB_SRC_PARTICLE;
+          s.type = tr.type;
+          s.amount = tr.E;
+          s.dr = tr.l;
+          s.scale = 1;
+        }
+        out[k] = s;
+      }
+      k++;
+    }
+    *n = k;
+    *lines = line;
   });
 }
 

@@ -177,6 +177,7 @@ void Engine::reset_streams() {
 void Engine::free_device(DeviceCtx& g) {
   cudaSetDevice(g.dev);
   g.back.reset();
+  g.front.reset();
   if (g.st) cudaStreamSynchronize(g.st);
   if (g.cp) cudaStreamSynchronize(g.cp);
   void* ptrs[] = {g.absca, g.wmeta, g.lp, g.oms, g.az, g.sc, g.lr, g.ls, g.is, g.mcol, g.bfrt, g.rs, g.rm};

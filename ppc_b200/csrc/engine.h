@@ -28,6 +28,7 @@ struct RunInfo {
 };
 
 struct BackendTables;  // the device back end's sensor tables (backend.cu)
+struct FrontScratch;   // the device front end's per-source buffers (frontend.cu)
 
 struct DeviceCtx {
   int dev = -1;
@@ -69,6 +70,7 @@ struct DeviceCtx {
   ppcb_hit* hhits = nullptr;       // pinned, grows
   uint64_t hhits_cap = 0;
   std::shared_ptr<BackendTables> back;  // built on the first device back-end call
+  std::shared_ptr<FrontScratch> front;  // grows to the largest device front-end call
 };
 
 struct GradScratch;  // the gradient's device buffers (gradient.cu), kept between calls
@@ -126,6 +128,11 @@ class Engine {
   // (device pointer), on stream st.  Standard sensors only.
   void accept(int d, const ppcb_hit* dhits, uint64_t n, uint32_t seed, ppcb_acc_hit* dout,
               unsigned long long* dcount, cudaStream_t st);
+  // Device front end on device `d`: sources to bunches (gpu/f2k.cxx:17-167, 377-528),
+  // one random stream per source; counts[0..1] (device) receive bunches needed and photons.
+  void sources(int d, const ppcb_source* dsrc, uint64_t ns, uint32_t seed, ppcb_bunch* dout, uint64_t* dbstart,
+               uint64_t cap, uint64_t* dcounts, cudaStream_t st);
+  int front_errors(int d);  // sources whose sampling failed, since ini (synchronises)
   // The back end's tables on device `d` (built from the configuration on first use).
   BackendTables& backend_tables(int d);
   double total_device_ms() const;

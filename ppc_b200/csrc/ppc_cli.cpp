@@ -59,27 +59,14 @@ void list_devices() {
 // f2k reader: one segment per input line, TR records become sources (gpu/f2k.cxx:555-583)
 void f2k(Session& s) {
   std::string in;
-  const float fcv = PPCB_FPI / 180.f;
   while (std::getline(std::cin, in)) {
     s.sett_line(in);
-    char name[32];
-    int gens, igen, type = -1;
-    float x, y, z, th, ph, l, E, t;
-    if (sscanf(in.c_str(), "TR %d %d %31s %f %f %f %f %f %f %f %f", &gens, &igen, name, &x, &y, &z, &th, &ph, &l,
-               &E, &t) == 11) {
-      th = fcv * (180 - th);
-      ph = fcv * (ph < 180 ? ph + 180 : ph - 180);
-      float costh = cosf(th), sinth = sinf(th), cosph = cosf(ph), sinph = sinf(ph);
+    F2kTrack tr;
+    if (parse_f2k_track(in, tr)) {
       s.p.q = s.flne;
-      s.p.n[0] = sinth * cosph; s.p.n[1] = sinth * sinph; s.p.n[2] = costh;
-      if (!strcmp(name, "amu+") || !strcmp(name, "amu-") || !strcmp(name, "amu")) type = 0;
-      else if (!strcmp(name, "delta") || !strcmp(name, "brems") || !strcmp(name, "epair") || !strcmp(name, "e"))
-        type = 11;
-      else if (!strcmp(name, "e-")) type = 12;
-      else if (!strcmp(name, "e+")) type = 13;
-      else if (!strcmp(name, "munu") || !strcmp(name, "hadr")) type = 101;
-      else if (!strcmp(name, "ph")) s.addf(x, y, z, t, (unsigned long long)E);
-      if (type >= 0) s.addp(x, y, z, t, E, l, type);
+      s.p.n[0] = tr.n[0]; s.p.n[1] = tr.n[1]; s.p.n[2] = tr.n[2];
+      if (tr.type == -2) s.addf(tr.x, tr.y, tr.z, tr.t, (unsigned long long)tr.E);
+      else if (tr.type >= 0) s.addp(tr.x, tr.y, tr.z, tr.t, tr.E, tr.l, tr.type);
     }
   }
   s.eout();

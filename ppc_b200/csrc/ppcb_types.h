@@ -81,6 +81,26 @@ typedef struct ppcb_bunch {
   } u;
 } ppcb_bunch;
 
+// A light source for the device front end: one addp (particle type), addp_clst,
+// addp_mopo or f2k "ph" record with its segment's direction and id.
+typedef struct ppcb_source {
+  float r[4];      // x, y, z [m], t [ns]
+  float n[3];      // direction (the segment's direction, as sett sets it)
+  int32_t kind;    // PPCB_SRC_*
+  double amount;   // PARTICLE: energy [GeV]; CLST, POINT: photons; MOPO: light
+  float dr;        // PARTICLE, CLST: track length [m]; MOPO: length
+  int32_t type;    // PARTICLE: 0 muon, 1 muon end point, 10-14 EM, 101-107 hadron (addp)
+  float scale;     // PARTICLE: light scale (addp)
+  float beta;      // CLST, MOPO
+  float tau, fr;   // MOPO
+  uint32_t q;      // segment id echoed in the hits
+  uint32_t pad_;
+} ppcb_source;
+#define PPCB_SRC_PARTICLE 0  // addp, type >= 0 (gpu/f2k.cxx:484-504)
+#define PPCB_SRC_CLST 1      // addp_clst (gpu/f2k.cxx:507-518)
+#define PPCB_SRC_MOPO 2      // addp_mopo (gpu/f2k.cxx:520-528)
+#define PPCB_SRC_POINT 3     // f2k "ph": exact count at a point (gpu/f2k.cxx:478-482)
+
 typedef struct ppcb_line {
   int16_t n, max; // first DOM index, last DOM offset
   float x, y, r;  // string centre and search radius

@@ -47,6 +47,33 @@ float Session::grnd() {
   return a * sinf(2 * PPCB_FPI * xrnd());
 }
 
+// gpu/f2k.cxx:559-582: direction from the zenith and azimuth of the track (pointing back to
+// where it comes from), particle names to light-yield types
+bool parse_f2k_track(const std::string& line, F2kTrack& tr) {
+  char name[32];
+  int gens, igen;
+  float th, ph;
+  if (sscanf(line.c_str(), "TR %d %d %31s %f %f %f %f %f %f %f %f", &gens, &igen, name, &tr.x, &tr.y, &tr.z, &th,
+             &ph, &tr.l, &tr.E, &tr.t) != 11)
+    return false;
+  const float fcv = PPCB_FPI / 180.f;
+  th = fcv * (180 - th);
+  ph = fcv * (ph < 180 ? ph + 180 : ph - 180);
+  const float costh = cosf(th), sinth = sinf(th), cosph = cosf(ph), sinph = sinf(ph);
+  tr.n[0] = sinth * cosph;
+  tr.n[1] = sinth * sinph;
+  tr.n[2] = costh;
+  tr.type = -1;
+  if (!strcmp(name, "amu+") || !strcmp(name, "amu-") || !strcmp(name, "amu")) tr.type = 0;
+  else if (!strcmp(name, "delta") || !strcmp(name, "brems") || !strcmp(name, "epair") || !strcmp(name, "e"))
+    tr.type = 11;
+  else if (!strcmp(name, "e-")) tr.type = 12;
+  else if (!strcmp(name, "e+")) tr.type = 13;
+  else if (!strcmp(name, "munu") || !strcmp(name, "hadr")) tr.type = 101;
+  else if (!strcmp(name, "ph")) tr.type = -2;
+  return true;
+}
+
 // gpu/f2k.cxx:17-167: photons per bunch template for a source of energy E
 float Session::yield(float E, float dr, int type) {
   p.n[3] = dr;

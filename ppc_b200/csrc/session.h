@@ -16,6 +16,17 @@
 
 namespace ppcb {
 
+// One TR record of an f2k line (gpu/f2k.cxx:559-582): the source it makes (type >= 0 a
+// particle for addp, -2 an exact photon count "ph" for addf, -1 none), its position, time,
+// direction, length and energy.
+struct F2kTrack {
+  int type = -1;
+  float x = 0, y = 0, z = 0, t = 0, l = 0, E = 0;
+  float n[3] = {0, 0, 0};
+};
+// False when the line is not a TR record.
+bool parse_f2k_track(const std::string& line, F2kTrack& tr);
+
 class Session {
  public:
   Engine eng;

@@ -56,6 +56,23 @@ HIT_DTYPE = np.dtype([("i", "<u4"), ("n", "<u4"), ("z", "<u4"), ("t", "<f4"),
 ACC_DTYPE = np.dtype([("i", "<u4"), ("n", "<u4"), ("hit", "<u4"), ("str", "<i4"), ("om", "<i4"), ("pmt", "<i4"),
                       ("t", "<f4"), ("wv", "<f4"), ("r", "<f4", 3), ("d", "<f4", 3)])
 
+# a light source for the device front end (ppcb_source), 72 bytes
+SOURCE_DTYPE = np.dtype([("r", "<f4", 4), ("n", "<f4", 3), ("kind", "<i4"), ("amount", "<f8"), ("dr", "<f4"),
+                         ("type", "<i4"), ("scale", "<f4"), ("beta", "<f4"), ("tau", "<f4"), ("fr", "<f4"),
+                         ("q", "<u4"), ("pad_", "<u4")])
+SRC_PARTICLE, SRC_CLST, SRC_MOPO, SRC_POINT = 0, 1, 2, 3
+
+
+def source(kind, r, n=(0.0, 0.0, 1.0), amount=0.0, dr=0.0, type_=0, scale=1.0, beta=1.0, tau=0.0, fr=0.0, q=1):
+    """One source record: addp (SRC_PARTICLE: amount = E [GeV], type_), addp_clst
+    (SRC_CLST: amount = photons, beta), addp_mopo (SRC_MOPO: amount = light, dr = length,
+    beta, tau, fr) or an f2k "ph" point (SRC_POINT: amount = photons)."""
+    s = np.zeros(1, SOURCE_DTYPE)
+    s["r"], s["n"], s["kind"], s["amount"], s["dr"] = r, n, kind, amount, dr
+    s["type"], s["scale"], s["beta"], s["tau"], s["fr"], s["q"] = type_, scale, beta, tau, fr, q
+    return s
+
+
 # DirectFit likelihood records (ppcb_llh_hit / _window / _block), 24 bytes each
 LLH_HIT_DTYPE = np.dtype([("str", "<i4"), ("om", "<i4"), ("t", "<f8"), ("q", "<f8")])
 LLH_WINDOW_DTYPE = np.dtype([("str", "<i4"), ("om", "<i4"), ("ti", "<f8"), ("tf", "<f8")])

@@ -208,6 +208,7 @@ int main(void) {
   printf("ppcb_params %zu\\n", sizeof(ppcb_params));
   printf("ppcb_acc_hit %zu\\n", sizeof(ppcb_acc_hit));
   printf("ppcb_llh_hit %zu\\n", sizeof(ppcb_llh_hit));
+  printf("ppcb_source %zu\\n", sizeof(ppcb_source));
   printf("ppcb_llh_window %zu\\n", sizeof(ppcb_llh_window));
   printf("ppcb_llh_block %zu\\n", sizeof(ppcb_llh_block));
   printf("ppcb_llh_opts %zu\\n", sizeof(ppcb_llh_opts));
@@ -226,7 +227,7 @@ int main(void) {
           "ppcb_info": C.sizeof(_lib.Info), "ppcb_batch_info": C.sizeof(_lib.BatchInfo),
           "ppcb_tune_info": C.sizeof(_lib.TuneInfo), "ppcb_grad_info": C.sizeof(_lib.GradInfo),
           "ppcb_ctrl": C.sizeof(T.Ctrl), "ppcb_params": C.sizeof(T.Params), "ppcb_acc_hit": T.ACC_DTYPE.itemsize,
-          "ppcb_llh_hit": T.LLH_HIT_DTYPE.itemsize, "ppcb_llh_window": T.LLH_WINDOW_DTYPE.itemsize,
+          "ppcb_llh_hit": T.LLH_HIT_DTYPE.itemsize, "ppcb_source": T.SOURCE_DTYPE.itemsize, "ppcb_llh_window": T.LLH_WINDOW_DTYPE.itemsize,
           "ppcb_llh_block": T.LLH_BLOCK_DTYPE.itemsize, "ppcb_llh_opts": C.sizeof(_lib.LlhOpts),
           "ppcb_llh_info": C.sizeof(_lib.LlhInfo)}
     for k, v in py.items():
