@@ -104,6 +104,12 @@ int ppcb_addp_mopo(ppcb_ctx* c, float x, float y, float z, float t, float light,
 int ppcb_flone(ppcb_ctx* c, uint64_t num);                           /* flone(), gpu/f2k.cxx:586-588 */
 int ppcb_eout(ppcb_ctx* c);                                          /* eout(), gpu/f2k.cxx:536-541 */
 int ppcb_efin(ppcb_ctx* c);                                          /* efin(), gpu/f2k.cxx:544-546 */
+/* The host back end (print(), gpu/f2k.cxx:247-363) over kernel-level hits computed elsewhere,
+ * e.g. by ppcb_propagate_device: hits of the segments started with sett (segment ids in .n)
+ * go through acceptance, PMT choice and cable shadow into hitz.  Hits come in segment
+ * order: hits of a segment before the newest one already seen are dropped with the
+ * reference's "Internal Error" message.  No counterpart in the reference's API. */
+int ppcb_back_end(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n);
 int ppcb_set_res(ppcb_ctx* c, float t, float cz);                    /* set_res(), gpu/f2k.cxx:202-210 */
 float ppcb_xrnd(ppcb_ctx* c);                                        /* xrnd(), gpu/f2k.cxx:1-6 */
 

@@ -20,6 +20,11 @@
 //      in: (f32 E, f32 dr, i32 type, f32 scale) per source; out: (f32 mean, f32 f, f32 a,
 //      f32 b, f32 length, f32 yield) per source -- the bunch template addp() makes and the
 //      Poisson mean it samples (gpu/f2k.cxx:17-167, 484-504)
+//   ref_harness backend <hits> <seed> <out>
+//      the reference's own back end (print, gpu/f2k.cxx:247-363) over kernel-level hit
+//      records of one segment (n = 1, sett id (3, 9)), with the host random state sv = seed;
+//      out: the hit map, one 80-byte record per photon (track, str, om, pmt, dir, time,
+//      r[4], n[4]) in the map's order
 //   ref_harness run <spec> <photons> <seed> <out-prefix> [nodump]
 //      spec = "flasher:<str>:<om>" | "cascade:<x>:<y>:<z>:<E>:<nx>:<ny>:<nz>:<type>"
 //           | "point:<x>:<y>:<z>"   (isotropic point source, FWID=-1 style, at x,y,z)
@@ -153,6 +158,51 @@ int main(int argc, char** argv) {
     f = xopen(argv[3], "wb");
     fwrite(out.data(), sizeof(float), out.size(), f);
     fclose(f);
+    return 0;
+  }
+  if (mode == "backend" && argc >= 5) {
+    std::vector<hit> in;
+    {
+      FILE* f = xopen(argv[2], "rb");
+      hit h;
+      while (fread(&h, sizeof(hit), 1, f) == 1) in.push_back(h);
+      fclose(f);
+    }
+    initialize();
+    choose(0);
+    ini();
+    sv = strtoul(argv[3], 0, 10);
+    sett(0, 0, 1, std::make_pair(3, 9ULL), 0);
+    if (in.size() > d.hnum) { fprintf(stderr, "too many hits for one batch\n"); return 2; }
+    std::copy(in.begin(), in.end(), q.hits);
+    d.hidx = in.size();
+    print();
+    struct {
+      int first, frame;
+      unsigned long long second;
+      double t0;
+      int str, dom, pmt;
+      float dir, time, r[4], n[4];
+      unsigned int pad;
+    } rec;
+    FILE* f = xopen(argv[4], "wb");
+    for (std::map<ihit, std::vector<pout> >::const_iterator i = hitz.begin(); i != hitz.end(); ++i)
+      for (std::vector<pout>::const_iterator j = i->second.begin(); j != i->second.end(); ++j) {
+        memset(&rec, 0, sizeof(rec));
+        rec.first = i->first.track.first;
+        rec.second = i->first.track.second;
+        rec.frame = i->first.track.frame;
+        rec.t0 = i->first.track.t0;
+        rec.str = i->first.omkey.str;
+        rec.dom = i->first.omkey.dom;
+        rec.pmt = i->first.pmt;
+        rec.dir = i->first.dir;
+        rec.time = i->first.time;
+        for (int k = 0; k < 4; k++) rec.r[k] = j->r[k], rec.n[k] = j->n[k];
+        fwrite(&rec, sizeof(rec), 1, f);
+      }
+    fclose(f);
+    fin();
     return 0;
   }
   if (mode == "run" && argc >= 6) {

@@ -80,7 +80,7 @@ EXPORTS = [
     "ppcb_batch_hits", "ppcb_batch_autotune", "ppcb_set_ice", "ppcb_get_ice", "ppcb_gradient",
     "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept", "ppcb_llh_default_opts", "ppcb_llh_create",
     "ppcb_llh_destroy", "ppcb_llh_get_info", "ppcb_llh_blocks", "ppcb_llh_eval_device", "ppcb_llh_eval",
-    "ppcb_sources_device", "ppcb_sources", "ppcb_f2k_sources",
+    "ppcb_sources_device", "ppcb_sources", "ppcb_f2k_sources", "ppcb_back_end",
 ]
 
 
@@ -114,6 +114,7 @@ def lib():
         "ppcb_flone": (i32, [vp, u64]),
         "ppcb_eout": (i32, [vp]),
         "ppcb_efin": (i32, [vp]),
+        "ppcb_back_end": (i32, [vp, vp, u64]),
         "ppcb_set_res": (i32, [vp, f32, f32]),
         "ppcb_xrnd": (f32, [vp]),
         "ppcb_hitz_count": (i32, [vp, P(u64)]),

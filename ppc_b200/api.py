@@ -122,6 +122,12 @@ class PPC:
     def efin(self):
         check(lib().ppcb_efin(self._c))
 
+    def back_end(self, hits):
+        """The host back end over kernel-level hits computed elsewhere (ppcb_back_end): hits
+        of the segments started with sett go into hitz, in segment order."""
+        hits = np.ascontiguousarray(hits, T.HIT_DTYPE)
+        check(lib().ppcb_back_end(self._c, _p(hits) if len(hits) else None, len(hits)))
+
     def set_res(self, t, c=0.0):
         check(lib().ppcb_set_res(self._c, float(t), float(c)))
 

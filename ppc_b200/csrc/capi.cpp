@@ -167,6 +167,15 @@ int ppcb_eout(ppcb_ctx* c) {
   return guard([&] { c->s.eout(); });
 }
 
+int ppcb_back_end(ppcb_ctx* c, const ppcb_hit* hits, uint64_t n) {
+  CTX_OR_FAIL(c);
+  if (n > 0 && !hits) { g_err = "null argument"; return PPCB_EARG; }
+  return guard([&] {
+    std::vector<ppcb_hit> v(hits, hits + n);
+    c->s.print(v, c->s.flne);
+  });
+}
+
 int ppcb_efin(ppcb_ctx* c) {
   CTX_OR_FAIL(c);
   return guard([&] { c->s.efin(); });

@@ -12,7 +12,11 @@ Workloads (sizes as used by the tests and the benchmark):
           DOMs each (5160), 171 layers of 10 m with smooth log-normal (sigma 0.3) b_e and
           a_dust profiles, 1-d tilt with a +-20 m sinusoidal dust-layer shift, absorption
           anisotropy of strength 0.08, birefringence diffusion; HG/SAM mix as in SPICE.
-  full2d  the `full` detector and ice with a 2-d tilt map (tilt.set/tilt.map) instead.
+  full2d  the `full` detector and ice with a 2-d tilt map (tilt.set/tilt.map) instead,
+          sensor axes a few degrees off vertical (cx.dat) and cable azimuths (dx.dat).
+  full_ng the `full` configuration with multi-PMT sensors on strings 1-45 (om.conf,
+          om.map, om.dirs, om.wv_*): 24-PMT spheres, 2-PMT spheroids and wavelength-
+          shifting tubes, plus sensor axes and cable azimuths.
 
 The ice-model constants (alpha, kappa, A, B of icemodel.par, the 12 birefringence
 parameters of cfg.txt) are values of the same form and magnitude as the published SPICE
@@ -104,8 +108,8 @@ _BFR = [0.0768, 5.4e5, 2.23, 0.00262, 0.0774, 1.55e6, 2.45, 0.00250, 0.00100, 0.
 
 
 def write(kind, path, count=131072, xR=5):
-    """Writes configuration `kind` (small | small_tilt | small_hole | full | full2d) into
-    directory `path`."""
+    """Writes configuration `kind` (small | small_tilt | small_hole | full | full2d |
+    full_ng) into directory `path`."""
     os.makedirs(path, exist_ok=True)
     shutil.copyfile(multipliers_file(count), os.path.join(path, "rnd.txt"))
     with open(os.path.join(path, "icemodel.par"), "w") as f:
@@ -157,7 +161,47 @@ def write(kind, path, count=131072, xR=5):
         _sensor_axes_and_cables(path, np.random.default_rng(7))
     else:
         _tilt1d(path, rng)
+    if kind == "full_ng":
+        _sensor_axes_and_cables(path, np.random.default_rng(8))
+        _nextgen(path)
     return path
+
+
+def _nextgen(path):
+    """Multi-PMT sensors (om.conf, om.map, om.dirs, om.wv_<type>.0): strings 1-20 carry a
+    24-PMT sphere, 21-35 a 2-PMT elongated spheroid, 36-45 a wavelength-shifting tube
+    (a cylinder read out at both ends); the other strings keep standard DOMs."""
+    with open(os.path.join(path, "om.conf"), "w") as f:
+        f.write("msphere 1 0.0044 0.33 0.178 0.178 24 33.0 0.0 0.0\n")
+        first = True
+        for th, off in ((33.0, 0.0), (72.0, 30.0), (108.0, 0.0), (147.0, 30.0)):
+            for k in range(6):
+                if first:
+                    first = False
+                    continue
+                f.write(f"{th} {off + 60.0 * k}\n")
+        f.write("spheroid 2 0.010 0.33 0.15 0.27 2 0.0 0.0 15.0\n180.0 0.0\n")
+        f.write("tube 3 0.020 -2 0.057 -0.45 1 0.0 0.0\n")
+    with open(os.path.join(path, "om.map"), "w") as f:
+        for s in range(1, 46):
+            m = 1 if s <= 20 else 2 if s <= 35 else 3
+            for om in range(1, 61):
+                f.write(f"{s} {om} {m}\n")
+    n = 642  # Fibonacci sphere
+    k = np.arange(n) + 0.5
+    z = 1 - 2 * k / n
+    phi = np.pi * (1 + 5 ** 0.5) * k
+    rxy = np.sqrt(1 - z * z)
+    with open(os.path.join(path, "om.dirs"), "w") as f:
+        for i in range(n):
+            f.write(f"{i} {rxy[i] * np.cos(phi[i]):.7f} {rxy[i] * np.sin(phi[i]):.7f} {z[i]:.7f}\n")
+    # acceptance curves scaled so that each module type registers a fraction of the light
+    # comparable to a standard DOM's (integrated acceptance about 0.4-0.8 of it)
+    for m, (peak, width, top) in {1: (400.0, 90.0, 18000.0), 2: (390.0, 80.0, 3600.0),
+                                  3: (360.0, 60.0, 2100.0)}.items():
+        with open(os.path.join(path, f"om.wv_{m}.0"), "w") as f:
+            for w in np.arange(300.0, 601.0, 10.0):
+                f.write(f"{w:.1f} {top * np.exp(-0.5 * ((w - peak) / width) ** 2):.4f}\n")
 
 
 def _sensor_axes_and_cables(path, rng):

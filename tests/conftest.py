@@ -39,6 +39,11 @@ def ice_full2d():
 
 
 @pytest.fixture(scope="session")
+def ice_full_ng():
+    return _ice("full_ng")
+
+
+@pytest.fixture(scope="session")
 def ice_small_tilt():
     return _ice("small_tilt")
 

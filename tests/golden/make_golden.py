@@ -8,6 +8,9 @@ oracle/_ref/ref_harness) on the synthetic configurations of ppc_b200/synth.py an
   zshift_<kind>.npz     tilt shift and layer thickness at fixed random points
   run_<case>.npz        kernel-level hits, a digest of the phase-1 photon records and the
                         final random-stream state of a fixed-seed propagation
+  backend_<case>.npz    the reference's own back end (print, gpu/f2k.cxx:247-363) over the
+                        kernel-level hits of a propagation: its input hits, host seed and the
+                        hit map it fills
 
 Needs /root/reference (run in the build container):
     python tests/golden/make_golden.py [names...]   (configurations / cases; default all)
@@ -38,8 +41,32 @@ RUNS = [
     ("full2d_flasher", "full2d", "flasher:40:30", 20000, 7, {}),
     ("small_tilt_led", "small_tilt", "flasher:1:30", 20000, 9, {"FWID": "9.7"}),
     ("small_hole_point", "small_hole", "point:0:0:0", 20000, 11, {"FWID": "-1", "WFLA": "405"}),
+    ("full_ng_cascade", "full_ng", "cascade:-50:310:50:2000:0.3:0.4:0.8660254:11", 20000, 5, {}),
 ]
-KINDS = ("small", "full", "full2d", "small_tilt", "small_hole")
+KINDS = ("small", "full", "full2d", "small_tilt", "small_hole", "full_ng")
+
+# (case, configuration, source spec, photons, propagation seed, back-end seed): standard
+# sensors with cables and tilted axes; 24-PMT spheres, 2-PMT spheroids, shifting tubes
+BACKENDS = [
+    ("full2d", "full2d", "cascade:20:-60:-100:2000:0.3:0.4:0.8660254:11", 300000, 5, 77),
+    ("full_ng_sphere", "full_ng", "cascade:20:-60:-100:2000:0.3:0.4:0.8660254:11", 300000, 5, 78),
+    ("full_ng_spheroid", "full_ng", "cascade:-50:310:50:2000:0.3:0.4:0.8660254:11", 300000, 6, 79),
+    ("full_ng_tube", "full_ng", "cascade:-360:10:0:2000:0.3:0.4:0.8660254:11", 300000, 7, 80),
+]
+
+
+def dtmn_order(hits):
+    """The reference's deterministic back-end order (segment, DOM, time, wavelength bin;
+    gpu/f2k.cxx:236-244 with DTMN)."""
+    return hits[np.lexsort((hits["z"], hits["t"], hits["i"], hits["n"]))]
+
+
+def reference_back_end(icedir, hits, seed, tmp):
+    from ppc_b200._lib import HITZ_DTYPE
+    fi, fo = os.path.join(tmp, "bh.bin"), os.path.join(tmp, "bo.bin")
+    hits.tofile(fi)
+    O.run_harness(["backend", fi, str(seed), fo], {"PPCTABLESDIR": icedir + "/"})
+    return np.fromfile(fo, HITZ_DTYPE)
 
 
 def ice(kind):
@@ -91,6 +118,15 @@ def main(only=()):
                             rs=np.uint64(info["rs"]), seed=np.uint32(seed), photons=np.uint32(photons),
                             env=np.frombuffer(json.dumps(env).encode(), np.uint8))
         print(case, info)
+    for case, kind, spec, photons, seed, bseed in BACKENDS:
+        name = "backend_" + case
+        if only and name not in only:
+            continue
+        info, hits, _, _ = O.harness_run(ice(kind), spec, photons, seed, os.path.join(tmp, name))
+        hits = dtmn_order(hits)
+        out = reference_back_end(ice(kind), hits, bseed, tmp)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), hits=hits, seed=np.uint32(bseed), hitz=out)
+        print(name, len(hits), "hits ->", len(out), "records")
 
 
 if __name__ == "__main__":
