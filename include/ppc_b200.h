@@ -239,9 +239,9 @@ int ppcb_propagate_noalloc(ppcb_ctx* c, int device, const ppcb_bunch* bunches, i
 /* ---- hit back end on the device ----
  * The reference's back end runs on the host inside eout() (gpu/f2k.cxx:247-363); these
  * apply the same acceptance to kernel-level hits on the GPU: the wavelength x RDE
- * acceptance of the DOM's (module type, variant), the sensor's angular acceptance (standard
- * sensors; others are rejected with PPCB_EARG), the cable shadow, and a wavelength sampled
- * in the hit's bin.  Each hit draws from its own random stream keyed by (seed, hit index)
+ * acceptance of the DOM's (module type, variant), the sensor's PMT choice (getPMT: standard
+ * DOMs, multi-PMT modules, wavelength-shifting tubes with their transit delay added to the
+ * time), the cable shadow, and a wavelength sampled in the hit's bin.  Each hit draws from its own random stream keyed by (seed, hit index)
  * instead of the host's shared sequence: the same decisions in distribution, not hit by
  * hit.  Accepted hits are written in input order.
  * ppcb_accept_device: device pointers on `stream`; *count (a device pointer) receives the

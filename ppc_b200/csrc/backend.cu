@@ -2,9 +2,11 @@
 // to kernel-level hits on the GPU.  For every hit, in the reference's order of decisions:
 //   1. wavelength x RDE acceptance: a DOM with high voltage and an acceptance table for its
 //      (module type, variant) keeps the hit with probability rat[z] x rde / rmax;
-//   2. sensor angular acceptance (standard sensors, gpu/ini.cxx:237-247): polynomial in the
-//      cosine between the photon direction and the sensor axis against mas x u, or the
-//      impact point's height along the axis against a threshold;
+//   2. the sensor's PMT choice (getPMT, gpu/ini.cxx:210-280): for a standard DOM a
+//      polynomial in the cosine between the photon direction and the sensor axis against
+//      mas x u, or the impact point's height along the axis against a threshold; for a
+//      multi-PMT module one PMT by its angular response; for a wavelength-shifting tube the
+//      readout end and its transit delay (backend.cuh);
 //   3. cable shadow (gpu/f2k.cxx:314-335);
 //   4. wavelength sampled uniformly in the hit's wavelength bin.
 // The reference draws the three uniform numbers from one host stream in hit order; here
@@ -79,7 +81,7 @@ BackArgs back_args(Engine& e, int d, const ppcb_hit* dhits, uint64_t n, uint32_t
   BackendTables& T = e.backend_tables(d);
   const DeviceCtx& g = e.devs.at(d);
   BackArgs A;
-  A.hits = dhits; A.n = n; A.doms = T.doms; A.sensors = T.sensors; A.rat = T.rat; A.wvs = T.wvs;
+  A.hits = dhits; A.n = n; A.doms = T.doms; A.sensors = T.sensors; A.rat = T.rat; A.wvs = T.wvs; A.dirs = T.dirs;
   A.rm = g.rm; A.nmul = (uint32_t)std::max(1, std::min(g.T, 1024)); A.seed = seed; A.gsize = e.cfg.p.gsize;
   return A;
 }
@@ -90,6 +92,7 @@ BackendTables& Engine::backend_tables(int d) {
   const Config& c = cfg;
   std::vector<BackDom> doms(c.p.gsize);
   std::vector<BackSensor> sensors;
+  std::vector<float3> pmt_dirs;
   std::map<int, int> sensor_index;
   std::vector<float> rat;
   std::map<std::pair<int, int>, int> acc_index;
@@ -122,17 +125,31 @@ BackendTables& Engine::backend_tables(int d) {
     auto ti = c.types.find(n.omt);
     if (ti != c.types.end()) {
       const SensorType& T = ti->second;
-      if (T.beta == -2 || !T.def || (int)T.s.size() > kMaxPoly)
-        throw Error("the device back end handles standard sensors only (module type " + std::to_string(n.omt) +
-                    " is not one); use the host back end (eout)", 7);
       auto si = sensor_index.find(n.omt);
       if (si == sensor_index.end()) {
         si = sensor_index.insert(std::make_pair(n.omt, (int)sensors.size())).first;
         BackSensor S{};
-        S.mas = T.mas;
-        S.ns = (int)T.s.size();
-        for (int i = 0; i < S.ns; i++) S.s[i] = T.s[i];
-        if (S.ns == 0) { S.ns = 1; S.s[0] = T.mas > 0 ? 0.f : 1.f; }
+        S.beta = T.beta;
+        S.fx = T.fx;
+        S.Rr = T.Rr;
+        S.Rz = T.Rz;
+        S.cable = T.cable;
+        if (T.beta == -2) {  // the getPMT branches in the reference's order (gpu/ini.cxx:210-280)
+          S.kind = kSensorTube;
+        } else if (T.def) {
+          if ((int)T.s.size() > kMaxPoly)
+            throw Error("the device back end takes angular polynomials of at most 16 coefficients", 7);
+          S.kind = kSensorStandard;
+          S.mas = T.mas;
+          S.ns = (int)T.s.size();
+          for (int i = 0; i < S.ns; i++) S.s[i] = T.s[i];
+          if (S.ns == 0) { S.ns = 1; S.s[0] = T.mas > 0 ? 0.f : 1.f; }
+        } else {
+          S.kind = kSensorMultiPMT;
+          S.dir0 = (int)pmt_dirs.size();
+          S.ndir = (int)T.dirs.size();
+          for (const Vec3& v : T.dirs) pmt_dirs.push_back(make_float3(v[0], v[1], v[2]));
+        }
         sensors.push_back(S);
       }
       D.sensor = si->second;
@@ -148,6 +165,9 @@ BackendTables& Engine::backend_tables(int d) {
   check(cudaMalloc((void**)&T->sensors, sensors.size() * sizeof(BackSensor)), "back end tables");
   check(cudaMalloc((void**)&T->rat, rat.size() * sizeof(float)), "back end tables");
   check(cudaMalloc((void**)&T->wvs, wvs.size() * sizeof(float2)), "back end tables");
+  if (pmt_dirs.empty()) pmt_dirs.push_back(make_float3(0, 0, 1));
+  check(cudaMalloc((void**)&T->dirs, pmt_dirs.size() * sizeof(float3)), "back end tables");
+  check(cudaMemcpy(T->dirs, pmt_dirs.data(), pmt_dirs.size() * sizeof(float3), cudaMemcpyHostToDevice), "H2D");
   check(cudaMemcpy(T->doms, doms.data(), doms.size() * sizeof(BackDom), cudaMemcpyHostToDevice), "H2D");
   check(cudaMemcpy(T->sensors, sensors.data(), sensors.size() * sizeof(BackSensor), cudaMemcpyHostToDevice), "H2D");
   check(cudaMemcpy(T->rat, rat.data(), rat.size() * sizeof(float), cudaMemcpyHostToDevice), "H2D");

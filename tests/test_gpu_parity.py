@@ -220,6 +220,11 @@ def _stat_sources():
                                                        a=2.01849 + 0.63176 * np.log(1e4),
                                                        b=0.39652 * 0.910 / 0.9216 / 0.63207), 4_000_000, 200_000
     yield "full_led_12fold", "full", None, 4_000_000, 200_000  # flasher on a DOM, built in the test
+    # multi-PMT modules: elongated spheroids (strings 21-35) and cylinders (strings 36-45)
+    for name, pos in (("full_ng_spheroids", [-50, 310, 50, 0]), ("full_ng_cylinders", [-360, 10, 0, 0])):
+        yield name, "full_ng", T.bunch_particle(pos, [0.3, 0.4, np.sqrt(0.75)], 1, 0, -11, f=0.0,
+                                                a=2.01849 + 0.63176 * np.log(1e4),
+                                                b=0.39652 * 0.910 / 0.9216 / 0.63207), 4_000_000, 200_000
 
 
 @pytest.mark.parametrize("name,kind,tmpl,ng,no", list(_stat_sources()), ids=[x[0] for x in _stat_sources()])

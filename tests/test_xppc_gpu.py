@@ -166,3 +166,67 @@ def test_device_back_end_matches_host_back_end(ice_full2d, monkeypatch):
         assert np.allclose(d["r"], h["r"][:3], atol=2e-5) and np.allclose(d["d"], h["n"][:3], atol=2e-5)
     assert ambiguous < 0.05 * len(host)
     assert both > 0.5 * min(len(host), len(dev)) * p_dev, (both, len(host), len(dev), p_dev)
+
+
+def _module_kind(s):
+    return np.where(s <= 20, 1, np.where(s <= 35, 2, np.where(s <= 45, 3, 0)))
+
+
+def test_device_back_end_multi_pmt_matches_host_back_end(ice_full_ng):
+    """Multi-PMT sensors on the device (24-PMT spheres, 2-PMT spheroids, shifting tubes)
+    against the host back end, which is pinned bit for bit to the reference's: accepted
+    fraction per module type, counts per (module type, PMT), and the tubes' transit delays."""
+    from scipy import stats
+    c = PPC()
+    c.initialize(1.0, ice_full_ng)
+    c.set_seed(8)
+    c.choose(0)
+    c.ini()
+    c.keep_raw(True)
+    raws, hosts = [], []
+    for e, (x, y, z) in enumerate([(20.0, -60.0, -100.0), (-50.0, 310.0, 50.0), (-360.0, 10.0, 0.0)] * 2):
+        c.sett(0.3, 0.4, 0.8660254, (e, 7), 0)
+        c.addp(x, y, z, 0.0, 20000.0, 0.0, 11)
+        c.eout()
+        hosts.append(c.hitz())
+        raws.append(c.raw_hits())
+        c.efin()
+    raw = np.concatenate(raws)
+    host = np.concatenate(hosts)
+    dev = c.accept(raw, seed=13)
+    c.close()
+    rs = raw["i"].astype(np.int64) // 60 + 1
+    rk, hk, dk = _module_kind(rs), _module_kind(host["str"]), _module_kind(dev["str"])
+    for k in (1, 2, 3):
+        n = int((rk == k).sum())
+        nh, nd = int((hk == k).sum()), int((dk == k).sum())
+        assert n > 3000 and nh > 500, (k, n, nh)
+        p = (nh + nd) / (2 * n)
+        assert abs(nh - nd) / n < 4 * np.sqrt(2 * p * (1 - p) / n), (k, n, nh, nd)
+    # PMT choice: counts per (module type, PMT)
+    cat_h = hk * 100 + host["pmt"]
+    cat_d = dk * 100 + dev["pmt"]
+    cats = np.union1d(cat_h, cat_d)
+    ch = np.array([np.count_nonzero(cat_h == x) for x in cats])
+    cd = np.array([np.count_nonzero(cat_d == x) for x in cats])
+    m = ch + cd >= 30
+    assert m.sum() >= 20
+    assert stats.chi2_contingency(np.vstack([ch[m], cd[m]]))[1] > 1e-3
+    # tubes: transit delays added to the hit time
+    tube = dk == 3
+    d_shift = dev["t"][tube] - raw["t"][dev["hit"][tube]]
+    assert np.all(d_shift > 0)
+    key = {}
+    for e, r in enumerate(raws):
+        s = r["i"].astype(np.int64) // 60 + 1
+        nz = np.cos(r["pth"]).astype(np.float32)
+        for j in np.nonzero(_module_kind(s) == 3)[0]:
+            key.setdefault((e, int(r["i"][j]), round(float(nz[j]), 4)), []).append(float(r["t"][j]))
+    h_shift = []
+    for h in host[hk == 3]:
+        ts = key.get((int(h["track_first"]), (int(h["str"]) - 1) * 60 + int(h["om"]) - 1, round(float(h["n"][2]), 4)))
+        if ts is not None and len(ts) == 1:
+            h_shift.append(float(h["r"][3]) - ts[0])
+    h_shift = np.array(h_shift)
+    assert len(h_shift) > 0.7 * (hk == 3).sum()
+    assert stats.ks_2samp(h_shift, d_shift).pvalue > 0.01
