@@ -141,6 +141,186 @@ def cpu_reference_sample(photons_per_proc, procs, seed=0):
     return {"value": rate, "photons": photons, "seconds": secs}
 
 
+def _ref_harness_json(args, ice, exe="ref_harness_fm"):
+    """One run of the reference harness (CPU build of the reference's own sources); its JSON
+    line, or None when the harness is not built."""
+    path = os.path.join(ROOT, "oracle", "_ref", exe)
+    if not os.path.exists(path):
+        return None
+    env = dict(os.environ, PPCTABLESDIR=ice + "/")
+    r = subprocess.run([path] + args, env=env, capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        return None
+    return json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+
+
+def _event_ms(fn, stream, reps, flush=None):
+    """Mean device time of fn() over reps calls, CUDA events on `stream`, L2 flushed before
+    each call when `flush` (a buffer larger than L2) is given."""
+    import torch
+    total = 0.0
+    for _ in range(reps):
+        if flush is not None:
+            flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total / reps
+
+
+def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps=5):
+    """The stages either side of the kernel, each on the GPU against the reference's (or the
+    oracle's) CPU code for the same work:
+      back end   ppcb_accept_device over the kernel-level hits of a 1e8-photon cascade on the
+                 2-d tilt detector with cables; CPU: the reference's own print() (one core)
+      likelihood ppcb_llh_eval_device, DirectFit's likelihood of those hits against the pulses
+                 of a 1e7-photon run of the same cascade, 64 time shifts per evaluation; CPU:
+                 the oracle's restatement (the reference's llh.cxx needs GSL), one core
+      front end  ppcb_sources_device over 1e6 mixed sources (muon segments, EM and hadronic
+                 cascades, 0.1-10 GeV); CPU: the reference's own addp() (one core)"""
+    import torch
+    from ppc_b200 import synth
+    from ppc_b200 import types as T
+    from ppc_b200.api import PPC, Likelihood
+
+    out = {}
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full2d")
+    if not os.path.exists(os.path.join(ice, "cfg.txt")):
+        synth.write("full2d", ice)
+    c = PPC()
+    c.initialize(1.0, ice)
+    c.set_seed(4242)
+    c.choose(local)
+    c.ini()
+    ppm = c.tables()["eff"][0]
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    hbm = _peaks().get("hbm_gbs")
+    rng = np.random.default_rng(99)
+    b = _cascade_bunch(rng, photons, q=1, ppm=ppm, fixed=[0.0, 0.0, 0.0, 0.3, 0.4, 0.8660254])[0]
+
+    def propagate(num, cap):
+        bb = b.copy()
+        bb["num"] = num
+        d_b = torch.from_numpy(bb.view(np.uint8).reshape(-1).copy()).cuda()
+        d_s = torch.tensor([0, num], dtype=torch.int64, device="cuda")
+        d_h = torch.empty((cap, 32), dtype=torch.uint8, device="cuda")
+        d_c = torch.zeros(56, dtype=torch.uint8, device="cuda")
+        c.propagate_device(d_b.data_ptr(), d_s.data_ptr(), 1, num, d_h.data_ptr(), cap, d_c.data_ptr(),
+                           stream.cuda_stream, 0)
+        torch.cuda.synchronize()
+        ctrl = T.Ctrl.from_buffer_copy(d_c.cpu().numpy().tobytes())
+        return d_h, min(int(ctrl.hidx), cap)
+
+    d_hits, nh = propagate(photons, 1 << 23)
+    raw = d_hits[:nh].cpu().numpy().view(T.HIT_DTYPE).reshape(-1)
+
+    # ---- back end
+    d_acc = torch.empty((max(1, nh), 56), dtype=torch.uint8, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    run = lambda: c.accept_device(d_hits.data_ptr(), nh, 7, d_acc.data_ptr(), d_cnt.data_ptr(), stream.cuda_stream,
+                                  0)
+    run()
+    torch.cuda.synchronize()
+    ms = _event_ms(run, stream, reps, flush)
+    acc = int(d_cnt.item())
+    algo = 32 * nh + 56 * acc
+    be = {"hits": nh, "accepted": acc, "device_ms": ms, "hits_per_s": nh / (ms / 1e3), "gpu_launches": 3,
+          "roofline": {"bound": "hbm", "achieved": algo / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                       "frac": (algo / (ms / 1e3) / 1e9) / hbm if hbm else None,
+                       "bytes": "32 B read per hit + 56 B written per accepted hit",
+                       "peak_source": "of measured (MEASURED_PEAKS.json)"}}
+    sample = raw[:100_000]
+    sample = sample[np.lexsort((sample["z"], sample["t"], sample["i"], sample["n"]))]
+    path = "/tmp/ppcb_stage_hits.bin"
+    sample.tofile(path)
+    r = _ref_harness_json(["backend", path, "77", "/tmp/ppcb_stage_hitz.bin"], ice)
+    if r:
+        be["cpu"] = {"hits_per_s": r["hits"] / r["seconds"], "cores": 1, "kind": "reference",
+                     "sample": f"{r['hits']} of the same hits through the reference's print() "
+                               "(oracle/_ref/ref_harness_fm backend)"}
+        be["speedup_vs_cpu"] = be["hits_per_s"] / be["cpu"]["hits_per_s"]
+    out["back_end"] = be
+
+    # ---- likelihood
+    d_small, ns = propagate(photons // 10, 1 << 22)
+    obs = c.accept(d_small[:ns].cpu().numpy().view(T.HIT_DTYPE).reshape(-1), seed=3)
+    data = np.zeros(len(obs), T.LLH_HIT_DTYPE)
+    data["str"], data["om"], data["t"], data["q"] = obs["str"], obs["om"], obs["t"], 1.0
+    L = Likelihood(c, data)
+    dts = np.linspace(-200.0, 200.0, shifts)
+    d_out = torch.empty(shifts, dtype=torch.float64, device="cuda")
+    run = lambda: L.eval_device(d_hits.data_ptr(), nh, dts, 10.0, d_out.data_ptr(), seed=5, stream=stream.cuda_stream)
+    run()
+    torch.cuda.synchronize()
+    ms = _event_ms(run, stream, reps, flush)
+    lk = {"hits": nh, "shifts": shifts, "doms": L.info()["doms"], "blocks": L.info()["blocks"], "device_ms": ms,
+          "evals_per_s": shifts / (ms / 1e3), "hit_shifts_per_s": nh * shifts / (ms / 1e3), "gpu_launches": 3}
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_util as O  # CPU baseline leg: the oracle restatement of llh.cxx
+        sim = c.accept(raw, seed=5)
+        t0 = time.perf_counter()
+        O.llh_fllh(data, sim, dts[:8], 10.0)
+        secs = time.perf_counter() - t0
+        lk["cpu"] = {"evals_per_s": 8 / secs, "cores": 1, "kind": "port",
+                     "sample": "8 shifts of the same evaluation through oracle/llh_oracle.c (DirectFit's "
+                               "llh.cxx needs GSL, absent here), accepted hits given"}
+        lk["speedup_vs_cpu"] = lk["evals_per_s"] / lk["cpu"]["evals_per_s"]
+    except Exception as e:  # the oracle library is a build product of oracle/Makefile
+        lk["cpu"] = {"unavailable": str(e)[:120]}
+    L.close()
+    out["likelihood"] = lk
+
+    # ---- front end
+    kinds = np.array([0, 11, 12, 13, 14, 101, 102, 105])
+    src = np.zeros(sources, T.SOURCE_DTYPE)
+    src["kind"] = T.SRC_PARTICLE
+    src["r"][:, :3] = rng.uniform(-400, 400, (sources, 3))
+    src["n"] = [0.3, 0.4, 0.8660254]
+    src["amount"] = 10 ** rng.uniform(-1, 1, sources)
+    src["type"] = rng.choice(kinds, sources)
+    src["dr"] = np.where(src["type"] == 0, rng.uniform(1, 20, sources), 0)
+    src["scale"] = 1
+    src["q"] = 1
+    d_src = torch.from_numpy(src.view(np.uint8).reshape(-1).copy()).cuda()
+    cap = sources + 1024
+    d_bun = torch.empty((cap, 64), dtype=torch.uint8, device="cuda")
+    d_bs = torch.empty(cap + 1, dtype=torch.int64, device="cuda")
+    d_fc = torch.zeros(2, dtype=torch.int64, device="cuda")
+    run = lambda: c.sources_device(d_src.data_ptr(), sources, 11, d_bun.data_ptr(), d_bs.data_ptr(), cap,
+                                   d_fc.data_ptr(), stream.cuda_stream, 0)
+    run()
+    torch.cuda.synchronize()
+    ms = _event_ms(run, stream, reps, flush)
+    nb, nph = (int(x) for x in d_fc.cpu().numpy())
+    algo = 72 * sources + 72 * nb
+    fe = {"sources": sources, "bunches": nb, "photons": nph, "device_ms": ms, "sources_per_s": sources / (ms / 1e3),
+          "gpu_launches": 3,
+          "roofline": {"bound": "hbm", "achieved": algo / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                       "frac": (algo / (ms / 1e3) / 1e9) / hbm if hbm else None,
+                       "bytes": "72 B read per source + 64 B bunch and 8 B start written per bunch",
+                       "peak_source": "of measured (MEASURED_PEAKS.json)"}}
+    fsrc = np.zeros(sources, [("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("t", "<f4"), ("E", "<f4"), ("dr", "<f4"),
+                              ("type", "<i4")])
+    fsrc["x"], fsrc["y"], fsrc["z"] = src["r"][:, 0], src["r"][:, 1], src["r"][:, 2]
+    fsrc["E"], fsrc["dr"], fsrc["type"] = src["amount"], src["dr"], src["type"]
+    fsrc.tofile("/tmp/ppcb_stage_sources.bin")
+    r = _ref_harness_json(["frontend", "/tmp/ppcb_stage_sources.bin", "5"], os.path.join(ROOT, "ppc_b200", "data",
+                                                                                      "ice", "full2d"))
+    if r:
+        fe["cpu"] = {"sources_per_s": r["sources"] / r["seconds"], "cores": 1, "kind": "reference",
+                     "sample": f"the same {r['sources']} sources through the reference's addp() "
+                               "(oracle/_ref/ref_harness_fm frontend)"}
+        fe["speedup_vs_cpu"] = fe["sources_per_s"] / fe["cpu"]["sources_per_s"]
+    out["front_end"] = fe
+    c.close()
+    return out
+
+
 def plain_kernel_sample(cascades, photons, local):
     """The reference's own CUDA kernel (gpu/pro.cu built for sm_100a with gpu/Makefile's
     flags, oracle/_ref/ref_gpu_harness) on the same cascades as the timed steps (vertex,
@@ -669,6 +849,8 @@ def run_ours(args, rank, world, local):
             torch.cuda.empty_cache()
             c.close()
         line["gradient"] = gradient_sample(local, plain_kernel=not args.no_plain_kernel)
+    if single and not args.no_stages:
+        line["stages"] = stages_sample(local)
     if single and not args.no_cpu_baseline:
         r = cpu_reference_sample(args.ref_photons, os.cpu_count() or 1)
         if r:
@@ -693,6 +875,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")
     ap.add_argument("--no-gradient", action="store_true", help="skip the ice-gradient evaluation")
+    ap.add_argument("--no-stages", action="store_true", help="skip the back end, likelihood and front end stages")
     ap.add_argument("--cascade", type=lambda t: [float(x) for x in t.split(",")], default=None,
                     help="x,y,z,nx,ny,nz: one fixed cascade for every step instead of random ones (profiling)")
     ap.add_argument("--config", default="cascade", choices=["cascade", "batched", "fit"],

@@ -25,6 +25,10 @@
 //      records of one segment (n = 1, sett id (3, 9)), with the host random state sv = seed;
 //      out: the hit map, one 80-byte record per photon (track, str, om, pmt, dir, time,
 //      r[4], n[4]) in the map's order
+//   ref_harness frontend <sources> <seed>
+//      times the reference's own front end (addp: yield, poidev, addh; gpu/f2k.cxx:17-167,
+//      377-504) over (f32 x, y, z, t, E, dr, i32 type) per source; the bunches are dropped
+//      before a batch fills, so no propagation runs.  Prints photons and seconds.
 //   ref_harness run <spec> <photons> <seed> <out-prefix> [nodump]
 //      spec = "flasher:<str>:<om>" | "cascade:<x>:<y>:<z>:<E>:<nx>:<ny>:<nz>:<type>"
 //           | "point:<x>:<y>:<z>"   (isotropic point source, FWID=-1 style, at x,y,z)
@@ -160,6 +164,31 @@ int main(int argc, char** argv) {
     fclose(f);
     return 0;
   }
+  if (mode == "frontend" && argc >= 4) {
+    struct { float x, y, z, t, E, dr; int type; } src;
+    std::vector<decltype(src)> in;
+    {
+      FILE* f = xopen(argv[2], "rb");
+      while (fread(&src, sizeof(src), 1, f) == 1) in.push_back(src);
+      fclose(f);
+    }
+    initialize();
+    choose(0);
+    ini();
+    sv = strtoul(argv[3], 0, 10);
+    sett(0.3f, 0.4f, 0.8660254f, std::make_pair(1, 1ULL), 0);
+    unsigned long long photons = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    for (size_t k = 0; k < in.size(); k++) {
+      addp(in[k].x, in[k].y, in[k].z, in[k].t, in[k].E, in[k].dr, in[k].type);
+      for (unsigned int j = 0; j < pk; j++) photons += q.pz[j].num;
+      pn = 0;  // drop the bunches: only the front end is timed
+      pk = 0;
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    printf("{\"sources\": %zu, \"photons\": %llu, \"seconds\": %.6f}\n", in.size(), photons, secs);
+    return 0;
+  }
   if (mode == "backend" && argc >= 5) {
     std::vector<hit> in;
     {
@@ -176,7 +205,10 @@ int main(int argc, char** argv) {
     if (in.size() > d.hnum) { fprintf(stderr, "too many hits for one batch\n"); return 2; }
     std::copy(in.begin(), in.end(), q.hits);
     d.hidx = in.size();
+    auto t0 = std::chrono::steady_clock::now();
     print();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    printf("{\"hits\": %zu, \"seconds\": %.6f}\n", in.size(), secs);
     struct {
       int first, frame;
       unsigned long long second;

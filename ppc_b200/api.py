@@ -348,6 +348,15 @@ def _accept(self, hits, seed=0):
 PPC.accept = _accept
 
 
+def _accept_device(self, hits_ptr, n, seed, out_ptr, count_ptr, stream=0, device=0):
+    """ppcb_accept_device over caller-owned device memory (raw pointers), asynchronous."""
+    check(lib().ppcb_accept_device(self._c, int(device), C.c_void_p(hits_ptr), int(n), int(seed) & 0xFFFFFFFF,
+                                   C.c_void_p(out_ptr), C.c_void_p(count_ptr), C.c_void_p(stream) if stream else None))
+
+
+PPC.accept_device = _accept_device
+
+
 def _sources(self, src, seed=0, cap=None):
     """Device front end (ppcb_sources): sources (SOURCE_DTYPE) to photon bunches, Poisson
     counts drawn on the GPU.  Returns (bunches, bstart, photons); bstart[k] is the first
@@ -366,6 +375,16 @@ def _sources(self, src, seed=0, cap=None):
 
 
 PPC.sources = _sources
+
+
+def _sources_device(self, src_ptr, ns, seed, out_ptr, bstart_ptr, cap, counts_ptr, stream=0, device=0):
+    """ppcb_sources_device over caller-owned device memory (raw pointers), asynchronous."""
+    check(lib().ppcb_sources_device(self._c, int(device), C.c_void_p(src_ptr), int(ns), int(seed) & 0xFFFFFFFF,
+                                    C.c_void_p(out_ptr), C.c_void_p(bstart_ptr), int(cap), C.c_void_p(counts_ptr),
+                                    C.c_void_p(stream) if stream else None))
+
+
+PPC.sources_device = _sources_device
 
 
 def f2k_sources(text, first_segment=1):

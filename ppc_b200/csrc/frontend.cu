@@ -6,8 +6,9 @@
 //   addp / addp_clst / addp_mopo / ph   gpu/f2k.cxx:478-528
 //   bunching                            gpu/f2k.cxx:377-385 (addh)
 // Three kernels: k_src_count (one thread per source: its bunch template, the light
-// fluctuation and the Poisson count, from the source's own random stream), k_src_scan (bunch
-// and photon offsets), k_src_write (the bunches and their first-photon indices).  A source
+// fluctuation and the Poisson count, from the source's own random stream; bunch and photon
+// totals per block of 256 sources), k_src_scan (offsets of the blocks), k_src_write (offsets
+// within the block by a CTA scan; the bunches and their first-photon indices).  A source
 // makes ceil(count / 2^31) bunches.  This file is compiled without fast-math and without
 // contraction, so the bunch templates follow the host front end's float arithmetic.
 #include <cuda_runtime.h>
@@ -22,13 +23,14 @@ namespace ppcb {
 
 struct FrontScratch {
   unsigned long long* num = nullptr;      // photons per source
-  unsigned long long* nrec = nullptr;     // bunches per source
-  unsigned long long* rec_off = nullptr;  // [ns + 1] first bunch of each source
-  unsigned long long* ph_off = nullptr;   // [ns + 1] first photon of each source
+  unsigned long long* blk_rec = nullptr;  // bunches per block of kThreads sources
+  unsigned long long* blk_ph = nullptr;   // photons per block
+  unsigned long long* rec_off = nullptr;  // [blocks + 1] first bunch of each block
+  unsigned long long* ph_off = nullptr;   // [blocks + 1] first photon of each block
   int* errors = nullptr;
   uint64_t cap = 0;
   ~FrontScratch() {
-    for (void* p : {(void*)num, (void*)nrec, (void*)rec_off, (void*)ph_off, (void*)errors})
+    for (void* p : {(void*)num, (void*)blk_rec, (void*)blk_ph, (void*)rec_off, (void*)ph_off, (void*)errors})
       if (p) cudaFree(p);
   }
 };
@@ -247,35 +249,77 @@ struct SrcArgs {
   uint32_t nmul, seed;
   float eff, ovr;
   unsigned long long* num;
-  unsigned long long* nrec;
+  unsigned long long* blk_rec;
+  unsigned long long* blk_ph;
   int* errors;
 };
 
-__global__ void __launch_bounds__(kThreads) k_src_count(SrcArgs A) {
-  const uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
-  if (k >= A.n) return;
-  const ppcb_source s = A.src[k];
-  SrcRng r = src_stream(A.seed, k, A.rm, A.nmul);
-  ppcb_bunch p;
-  bool err = false;
-  const double mean = src_bunch(s, A.eff, A.ovr, p, &r, err);
-  unsigned long long num;
-  if (mean < 0) {  // exact count
-    if (!(s.amount >= 0) || s.amount >= 1.8e19) {
-      err = true;
-      num = 0;
-    } else {
-      num = (unsigned long long)s.amount;
+// Exclusive prefix sums over the CTA of two per-thread values (warp shuffles, then the warp
+// totals); returns the CTA totals in *ta, *tb.
+__device__ void cta_scan2(unsigned long long& a, unsigned long long& b, unsigned long long* ta,
+                          unsigned long long* tb) {
+  __shared__ unsigned long long wa[kThreads / 32], wb[kThreads / 32];
+  const unsigned int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long ia = a, ib = b;
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long xa = __shfl_up_sync(0xffffffffu, ia, d), xb = __shfl_up_sync(0xffffffffu, ib, d);
+    if ((int)lane >= d) {
+      ia += xa;
+      ib += xb;
     }
-  } else {
-    num = src_poisson(mean, r, err);
   }
-  A.num[k] = num;
-  A.nrec[k] = (num + kMaxBunch - 1) / kMaxBunch;
-  if (err) atomicAdd(A.errors, 1);
+  if (lane == 31) {
+    wa[w] = ia;
+    wb[w] = ib;
+  }
+  __syncthreads();
+  unsigned long long oa = 0, ob = 0, sa = 0, sb = 0;
+  for (int j = 0; j < kThreads / 32; j++) {
+    if (j < (int)w) {
+      oa += wa[j];
+      ob += wb[j];
+    }
+    sa += wa[j];
+    sb += wb[j];
+  }
+  a = oa + ia - a;
+  b = ob + ib - b;
+  *ta = sa;
+  *tb = sb;
 }
 
-// exclusive scans of the bunch and photon counts (one block, a contiguous chunk per thread)
+__device__ __forceinline__ unsigned long long src_bunches(unsigned long long num) {
+  return (num + kMaxBunch - 1) / kMaxBunch;
+}
+
+__global__ void __launch_bounds__(kThreads) k_src_count(SrcArgs A) {
+  const uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+  unsigned long long num = 0;
+  if (k < A.n) {
+    const ppcb_source s = A.src[k];
+    SrcRng r = src_stream(A.seed, k, A.rm, A.nmul);
+    ppcb_bunch p;
+    bool err = false;
+    const double mean = src_bunch(s, A.eff, A.ovr, p, &r, err);
+    if (mean < 0) {  // exact count
+      if (!(s.amount >= 0) || s.amount >= 1.8e19) err = true;
+      else num = (unsigned long long)s.amount;
+    } else {
+      num = src_poisson(mean, r, err);
+    }
+    A.num[k] = num;
+    if (err) atomicAdd(A.errors, 1);
+  }
+  unsigned long long nr = src_bunches(num), np = num, tr, tp;
+  cta_scan2(nr, np, &tr, &tp);
+  if (threadIdx.x == 0) {
+    A.blk_rec[blockIdx.x] = tr;
+    A.blk_ph[blockIdx.x] = tp;
+  }
+}
+
+// exclusive scans of the blocks' bunch and photon totals (one block, a contiguous chunk of
+// blocks per thread)
 __global__ void k_src_scan(const unsigned long long* nrec, const unsigned long long* num, uint64_t n,
                            unsigned long long* rec_off, unsigned long long* ph_off, uint64_t* counts) {
   __shared__ unsigned long long pr[1024], pp[1024];
@@ -313,24 +357,30 @@ __global__ void k_src_scan(const unsigned long long* nrec, const unsigned long l
 }
 
 __global__ void __launch_bounds__(kThreads) k_src_write(SrcArgs A, const unsigned long long* rec_off,
-                                                        const unsigned long long* ph_off, ppcb_bunch* out,
-                                                        uint64_t* bstart, uint64_t cap) {
+                                                        const unsigned long long* ph_off, uint64_t nblk,
+                                                        ppcb_bunch* out, uint64_t* bstart, uint64_t cap) {
   const uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+  const unsigned long long num = k < A.n ? A.num[k] : 0, nrec = src_bunches(num);
+  unsigned long long b0 = nrec, ph0 = num, tr, tp;
+  cta_scan2(b0, ph0, &tr, &tp);
   if (k >= A.n) return;
-  const ppcb_source s = A.src[k];
-  ppcb_bunch p;
-  bool err = false;
-  src_bunch(s, A.eff, A.ovr, p, nullptr, err);
-  const unsigned long long num = A.num[k], b0 = rec_off[k], ph0 = ph_off[k];
-  for (unsigned long long j = 0; j < A.nrec[k]; j++) {
-    const unsigned long long b = b0 + j;
-    if (b >= cap) break;
-    const unsigned long long left = num - j * kMaxBunch;
-    p.num = (uint32_t)(left < kMaxBunch ? left : kMaxBunch);
-    out[b] = p;
-    bstart[b] = ph0 + j * kMaxBunch;
+  b0 += rec_off[blockIdx.x];
+  ph0 += ph_off[blockIdx.x];
+  if (nrec > 0) {
+    const ppcb_source s = A.src[k];
+    ppcb_bunch p;
+    bool err = false;
+    src_bunch(s, A.eff, A.ovr, p, nullptr, err);
+    for (unsigned long long j = 0; j < nrec; j++) {
+      const unsigned long long b = b0 + j;
+      if (b >= cap) break;
+      const unsigned long long left = num - j * kMaxBunch;
+      p.num = (uint32_t)(left < kMaxBunch ? left : kMaxBunch);
+      out[b] = p;
+      bstart[b] = ph0 + j * kMaxBunch;
+    }
   }
-  if (k == A.n - 1 && rec_off[A.n] <= cap) bstart[rec_off[A.n]] = ph_off[A.n];
+  if (k == A.n - 1 && rec_off[nblk] <= cap) bstart[rec_off[nblk]] = ph_off[nblk];
 }
 
 }  // namespace
@@ -354,16 +404,17 @@ void Engine::sources(int d, const ppcb_source* dsrc, uint64_t ns, uint32_t seed,
   }
   FrontScratch& F = *g.front;
   if (ns > F.cap) {
-    for (void** p : {(void**)&F.num, (void**)&F.nrec, (void**)&F.rec_off, (void**)&F.ph_off})
+    for (void** p : {(void**)&F.num, (void**)&F.blk_rec, (void**)&F.blk_ph, (void**)&F.rec_off, (void**)&F.ph_off})
       if (*p) {
         cudaFree(*p);
         *p = nullptr;
       }
     F.cap = 0;
     check(cudaMalloc((void**)&F.num, ns * sizeof(unsigned long long)), "front end scratch");
-    check(cudaMalloc((void**)&F.nrec, ns * sizeof(unsigned long long)), "front end scratch");
-    check(cudaMalloc((void**)&F.rec_off, (ns + 1) * sizeof(unsigned long long)), "front end scratch");
-    check(cudaMalloc((void**)&F.ph_off, (ns + 1) * sizeof(unsigned long long)), "front end scratch");
+    check(cudaMalloc((void**)&F.blk_rec, grid * sizeof(unsigned long long)), "front end scratch");
+    check(cudaMalloc((void**)&F.blk_ph, grid * sizeof(unsigned long long)), "front end scratch");
+    check(cudaMalloc((void**)&F.rec_off, (grid + 1) * sizeof(unsigned long long)), "front end scratch");
+    check(cudaMalloc((void**)&F.ph_off, (grid + 1) * sizeof(unsigned long long)), "front end scratch");
     F.cap = ns;
   }
   SrcArgs A;
@@ -375,13 +426,14 @@ void Engine::sources(int d, const ppcb_source* dsrc, uint64_t ns, uint32_t seed,
   A.eff = cfg.eff;
   A.ovr = cfg.ovr;
   A.num = F.num;
-  A.nrec = F.nrec;
+  A.blk_rec = F.blk_rec;
+  A.blk_ph = F.blk_ph;
   A.errors = F.errors;
   k_src_count<<<(unsigned int)grid, kThreads, 0, st>>>(A);
   check(cudaGetLastError(), "front end count");
-  k_src_scan<<<1, 1024, 0, st>>>(F.nrec, F.num, ns, F.rec_off, F.ph_off, dcounts);
+  k_src_scan<<<1, 1024, 0, st>>>(F.blk_rec, F.blk_ph, grid, F.rec_off, F.ph_off, dcounts);
   check(cudaGetLastError(), "front end scan");
-  k_src_write<<<(unsigned int)grid, kThreads, 0, st>>>(A, F.rec_off, F.ph_off, dout, dbstart, cap);
+  k_src_write<<<(unsigned int)grid, kThreads, 0, st>>>(A, F.rec_off, F.ph_off, grid, dout, dbstart, cap);
   check(cudaGetLastError(), "front end write");
 }
 
