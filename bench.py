@@ -186,7 +186,9 @@ def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps
     from ppc_b200 import types as T
     from ppc_b200.api import PPC, Likelihood
 
+    import tempfile
     out = {}
+    tmp = tempfile.mkdtemp(prefix="ppcb_stages_")
     ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full2d")
     if not os.path.exists(os.path.join(ice, "cfg.txt")):
         synth.write("full2d", ice)
@@ -235,9 +237,9 @@ def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps
                        "peak_source": "of measured (MEASURED_PEAKS.json)"}}
     sample = raw[:100_000]
     sample = sample[np.lexsort((sample["z"], sample["t"], sample["i"], sample["n"]))]
-    path = "/tmp/ppcb_stage_hits.bin"
+    path = os.path.join(tmp, "hits.bin")
     sample.tofile(path)
-    r = _ref_harness_json(["backend", path, "77", "/tmp/ppcb_stage_hitz.bin"], ice)
+    r = _ref_harness_json(["backend", path, "77", os.path.join(tmp, "hitz.bin")], ice)
     if r:
         be["cpu"] = {"hits_per_s": r["hits"] / r["seconds"], "cores": 1, "kind": "reference",
                      "sample": f"{r['hits']} of the same hits through the reference's print() "
@@ -308,9 +310,8 @@ def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps
                               ("type", "<i4")])
     fsrc["x"], fsrc["y"], fsrc["z"] = src["r"][:, 0], src["r"][:, 1], src["r"][:, 2]
     fsrc["E"], fsrc["dr"], fsrc["type"] = src["amount"], src["dr"], src["type"]
-    fsrc.tofile("/tmp/ppcb_stage_sources.bin")
-    r = _ref_harness_json(["frontend", "/tmp/ppcb_stage_sources.bin", "5"], os.path.join(ROOT, "ppc_b200", "data",
-                                                                                      "ice", "full2d"))
+    fsrc.tofile(os.path.join(tmp, "sources.bin"))
+    r = _ref_harness_json(["frontend", os.path.join(tmp, "sources.bin"), "5"], ice)
     if r:
         fe["cpu"] = {"sources_per_s": r["sources"] / r["seconds"], "cores": 1, "kind": "reference",
                      "sample": f"the same {r['sources']} sources through the reference's addp() "
@@ -318,6 +319,8 @@ def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps
         fe["speedup_vs_cpu"] = fe["sources_per_s"] / fe["cpu"]["sources_per_s"]
     out["front_end"] = fe
     c.close()
+    import shutil
+    shutil.rmtree(tmp, ignore_errors=True)
     return out
 
 
