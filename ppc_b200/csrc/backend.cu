@@ -59,9 +59,15 @@ __global__ void k_accept_scan(const unsigned int* cnt, uint64_t nb, unsigned lon
   if (t == nt - 1) off[nb] = part[t];
 }
 
+// The block's accepted records are compacted in shared memory, then copied out as one
+// contiguous run with coalesced 4-byte stores (a record is 14 words; the caller's buffer
+// needs only the record's own 4-byte alignment).
 __global__ void __launch_bounds__(kBlock) k_accept_write(BackArgs A, const unsigned long long* off,
                                                          ppcb_acc_hit* out) {
+  static_assert(sizeof(ppcb_acc_hit) == 56, "record of 14 words of 4 bytes");
+  constexpr int kWords = 14;
   __shared__ unsigned int warp_cnt[kBlock / 32];
+  __shared__ uint32_t stage[kBlock * kWords];
   const uint64_t k = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
   ppcb_acc_hit o;
   const bool f = k < A.n && accept_one(A, k, o);
@@ -69,9 +75,19 @@ __global__ void __launch_bounds__(kBlock) k_accept_write(BackArgs A, const unsig
   const unsigned int bal = __ballot_sync(0xffffffffu, f);
   if (lane == 0) warp_cnt[w] = __popc(bal);
   __syncthreads();
-  unsigned int before = 0;
-  for (unsigned int j = 0; j < w; j++) before += warp_cnt[j];
-  if (f) out[off[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u))] = o;
+  unsigned int before = 0, total = 0;
+  for (unsigned int j = 0; j < kBlock / 32; j++) {
+    if (j < w) before += warp_cnt[j];
+    total += warp_cnt[j];
+  }
+  if (f) {
+    const unsigned int pos = before + __popc(bal & ((1u << lane) - 1u));
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&o);
+    for (int q = 0; q < kWords; q++) stage[pos * kWords + q] = src[q];
+  }
+  __syncthreads();
+  uint32_t* dst = reinterpret_cast<uint32_t*>(out + off[blockIdx.x]);
+  for (unsigned int q = threadIdx.x; q < total * kWords; q += kBlock) dst[q] = stage[q];
 }
 
 }  // namespace

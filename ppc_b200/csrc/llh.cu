@@ -60,7 +60,7 @@ struct FillArgs {
   unsigned int* stot;
   unsigned long long* nohit;
   double t0, lbin;
-  int nblocks, ndom, ndt, unh;
+  int nblocks, ndom, ndt, unh, norm;
   double dt[PPCB_LLH_MAX_SHIFTS];
 };
 
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(kThreads) k_llh_fill(FillArgs F) {
         if (!(b >= D.n1 && b < D.n2)) continue;  // also drops NaN times
         const int blk = F.bin_block[D.bin0 + (int)b - D.n1];
         atomicAdd(&F.simc[(size_t)j * F.nblocks + blk], 1u);
-        atomicAdd(&F.stot[(size_t)j * F.ndom + slot], 1u);
+        if (F.norm) atomicAdd(&F.stot[(size_t)j * F.ndom + slot], 1u);  // only norm reads it
       }
     }
   }
@@ -275,6 +275,7 @@ void Likelihood::eval_device(const ppcb_hit* dhits, uint64_t n, uint32_t seed, c
     F.ndom = ndom;
     F.ndt = ndt;
     F.unh = opts.unh;
+    F.norm = opts.norm;
     for (int j = 0; j < PPCB_LLH_MAX_SHIFTS; j++) F.dt[j] = j < ndt ? dts[j] : 0.0;
     k_llh_fill<<<(unsigned int)grid, kThreads, 0, st>>>(F);
     check(cudaGetLastError(), "likelihood fill");
