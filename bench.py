@@ -830,7 +830,12 @@ def run_ours(args, rank, world, local):
                      "traffic_source": f"ncu dram__bytes_read+write per photon-step ({args.dram_bytes_per_step:.1f} B) "
                                        "on a 1e7-photon launch, scaled by this launch's photon-steps",
                      "hbm": {"achieved_gbs": traffic / (launch_ms / 1000.0) / 1e9,
-                             "peak_gbs": _peaks().get("hbm_gbs"), "peak_source": "of measured (MEASURED_PEAKS.json)"}},
+                             "peak_gbs": _peaks().get("hbm_gbs"), "peak_source": "of measured (MEASURED_PEAKS.json)"},
+                     # the binding limit, from the ncu capture of this kernel (not measured live):
+                     # issue slots busy and the FP32 (FMA), ALU and SFU (XU) pipes' share of peak
+                     "issue_ncu": {"issue_active": 0.846, "fma_pipe": 0.356, "alu_pipe": 0.437, "xu_pipe": 0.352,
+                                   "threads_per_warp_inst": 22.2,
+                                   "source": "profiles/k_propagate_cascade.md (ncu --set full, 1e7-photon cascade)"}},
         "clocks": clocks,
     }
     # the comparisons below are single-GPU figures: a multi-GPU run reports throughput only
