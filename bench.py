@@ -797,15 +797,28 @@ def run_ours(args, rank, world, local):
     e2e_value = world * photons * args.steps / e2e_total
     launch_ms = total_ms / args.steps
     steps_per_launch = steps_done / args.steps
-    # roofline: FP32.  FP32 operations per photon-step (thread-level FADD + FMUL + 2 x FFMA,
-    # counted by ncu on this kernel, profiles/k_propagate_cascade.md) x photon-steps of the
-    # launch / its event-timed duration, against the FFMA throughput measured on this GPU
-    # by the library's own FFMA loop (ppcb_fp32_peak).
-    from ppc_b200.api import fp32_peak
+    # roofline: FP32/SFU issue.  Per photon-step, the FP32 operations (thread-level FADD +
+    # FMUL + 2 x FFMA) and the special-function-unit thread instructions, both counted by ncu
+    # on this kernel and this workload's first cascade (profiles/k_propagate_roofline.md),
+    # x photon-steps of the launch / its event-timed duration; against the FFMA and SFU
+    # throughputs measured on this GPU by the library's own loops (ppcb_fp32_peak,
+    # ppcb_sfu_peak).  The roofline fraction is the larger of the two.
+    from ppc_b200.api import fp32_peak, sfu_peak
     ops_per_step = args.fp32_ops_per_step
     achieved = ops_per_step * steps_per_launch / (launch_ms / 1000.0) / 1e12
     props = torch.cuda.get_device_properties(local)
     peak = fp32_peak(local, repeats=5)
+    sfu_achieved = args.sfu_ops_per_step * steps_per_launch / (launch_ms / 1000.0) / 1e12
+    sfu_pk = sfu_peak(local, repeats=5)
+    fp32 = {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "ops_per_photon_step": ops_per_step,
+            "peak_source": f"measured: FFMA loop on all {props.multi_processor_count} SMs (ppcb_fp32_peak); "
+                           "no FP32 figure is among the driver-measured peaks"}
+    sfu = {"achieved": sfu_achieved, "peak": sfu_pk, "unit": "Tops/s", "frac": sfu_achieved / sfu_pk,
+           "ops_per_photon_step": args.sfu_ops_per_step,
+           "peak_source": f"measured: reciprocal-square-root loop on all {props.multi_processor_count} SMs "
+                          "(ppcb_sfu_peak)"}
+    top = sfu if sfu["frac"] > fp32["frac"] else fp32
     traffic = args.dram_bytes_per_step * steps_per_launch
     h2d = 64 + 16
     d2h = 32 * (e2e_hits / max(1, args.steps)) + 56
@@ -822,11 +835,11 @@ def run_ours(args, rank, world, local):
         "gpu_launches": args.steps,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h), "gpu_launches": args.steps},
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": f"measured: FFMA loop on all {props.multi_processor_count} SMs (ppcb_fp32_peak); "
-                                    "no FP32 figure is among the driver-measured peaks",
-                     "ops_per_photon_step": ops_per_step,
+        "roofline": {"bound": "sfu" if top is sfu else "fp32", "achieved": top["achieved"], "peak": top["peak"],
+                     "unit": top["unit"], "frac": top["frac"], "traffic": traffic,
+                     "peak_source": top["peak_source"],
+                     "kind": "FP32/SFU issue roofline: the larger of the FP32 and SFU fractions",
+                     "fp32": fp32, "sfu": sfu,
                      "traffic_source": f"ncu dram__bytes_read+write per photon-step ({args.dram_bytes_per_step:.1f} B) "
                                        "on a 1e7-photon launch, scaled by this launch's photon-steps",
                      "hbm": {"achieved_gbs": traffic / (launch_ms / 1000.0) / 1e9,
@@ -877,7 +890,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--photons", type=int, default=PHOTONS)
     ap.add_argument("--ref-photons", type=int, default=200_000)
-    ap.add_argument("--fp32-ops-per-step", type=float, default=405.5)
+    ap.add_argument("--fp32-ops-per-step", type=float, default=402.8)
+    ap.add_argument("--sfu-ops-per-step", type=float, default=50.6)
     ap.add_argument("--dram-bytes-per-step", type=float, default=0.007)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")

@@ -80,7 +80,7 @@ EXPORTS = [
     "ppcb_batch_hits", "ppcb_batch_autotune", "ppcb_set_ice", "ppcb_get_ice", "ppcb_gradient",
     "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept", "ppcb_llh_default_opts", "ppcb_llh_create",
     "ppcb_llh_destroy", "ppcb_llh_get_info", "ppcb_llh_blocks", "ppcb_llh_eval_device", "ppcb_llh_eval",
-    "ppcb_sources_device", "ppcb_sources", "ppcb_f2k_sources", "ppcb_back_end",
+    "ppcb_sources_device", "ppcb_sources", "ppcb_f2k_sources", "ppcb_back_end", "ppcb_sfu_peak",
 ]
 
 
@@ -143,6 +143,7 @@ def lib():
         "ppcb_get_ice": (i32, [vp, vp, vp, P(i32)]),
         "ppcb_gradient": (i32, [vp, vp, i32, u32, vp, vp, f64, u64, vp, vp, vp, P(GradInfo)]),
         "ppcb_fp32_peak": (i32, [i32, i32, P(f64), P(f64)]),
+        "ppcb_sfu_peak": (i32, [i32, i32, P(f64), P(f64)]),
         "ppcb_accept_device": (i32, [vp, i32, vp, u64, u32, vp, vp, vp]),
         "ppcb_accept": (i32, [vp, vp, u64, u32, vp, u64, P(u64)]),
         "ppcb_sources_device": (i32, [vp, i32, vp, u64, u32, vp, vp, u64, vp, vp]),

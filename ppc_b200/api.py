@@ -327,6 +327,13 @@ def _ice_methods():
 _ice_methods()
 
 
+def sfu_peak(device=0, repeats=5):
+    """Measured special-function-unit throughput of `device` in tera-ops/s (ppcb_sfu_peak)."""
+    t, ms = C.c_double(), C.c_double()
+    check(lib().ppcb_sfu_peak(int(device), int(repeats), C.byref(t), C.byref(ms)))
+    return t.value
+
+
 def fp32_peak(device=0, repeats=5):
     """Measured FP32 FMA throughput of `device` in TFLOP/s (ppcb_fp32_peak)."""
     t, ms = C.c_double(), C.c_double()

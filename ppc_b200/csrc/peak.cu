@@ -1,12 +1,15 @@
-// FP32 FMA throughput of the device (the denominator of the propagation kernel's FP32
-// roofline).  No counterpart in the reference.  Every thread runs 8 independent FFMA
-// chains so the FMA pipes stay full; the grid fills every SM at 1024 threads per SM.
+// FP32 FMA and SFU throughputs of the device (the denominators of the propagation kernel's
+// FP32/SFU issue roofline).  No counterpart in the reference.  Every thread runs 8
+// independent chains (FFMA, or reciprocal square roots on the special-function unit) so the
+// pipe stays full; the grid fills every SM at 1024 threads per SM.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <string>
 
 #include "../../include/ppc_b200.h"
+
+void ppcb_internal_set_error(const std::string& msg);
 
 namespace {
 
@@ -28,15 +31,29 @@ __global__ void __launch_bounds__(256) k_ffma(float* out, float a, float b) {
   if (s == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
 }
 
-}  // namespace
+// one reciprocal square root (MUFU.RSQ) and one FADD per link; the FADDs go to the FMA pipe,
+// four times faster than the special-function unit
+__global__ void __launch_bounds__(256) k_mufu(float* out, float b) {
+  float x[kChains];
+#pragma unroll
+  for (int k = 0; k < kChains; k++) x[k] = 1.f + threadIdx.x * 1e-3f + k;
+#pragma unroll 16
+  for (int i = 0; i < kIters; i++) {
+#pragma unroll
+    for (int k = 0; k < kChains; k++) x[k] = rsqrtf(x[k] + b);
+  }
+  float s = 0;
+#pragma unroll
+  for (int k = 0; k < kChains; k++) s += x[k];
+  if (s == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
+}
 
-void ppcb_internal_set_error(const std::string& msg);
-
-extern "C" int ppcb_fp32_peak(int device, int repeats, double* tflops, double* ms) {
-  if (!tflops || repeats <= 0) { ppcb_internal_set_error("ppcb_fp32_peak: bad argument"); return PPCB_EARG; }
+template <class L>
+int time_best(int device, int repeats, const char* who, L launch, double* best_ms) {
+  std::string tag(who);
   cudaDeviceProp p;
   if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&p, device) != cudaSuccess) {
-    ppcb_internal_set_error("ppcb_fp32_peak: no such device");
+    ppcb_internal_set_error(tag + ": no such device");
     return PPCB_ECUDA;
   }
   const int blocks = p.multiProcessorCount * 4, threads = 256;
@@ -48,7 +65,7 @@ extern "C" int ppcb_fp32_peak(int device, int repeats, double* tflops, double* m
   double best = 1e30;
   for (int r = 0; e == cudaSuccess && r < repeats + 2; r++) {
     cudaEventRecord(e0);
-    k_ffma<<<blocks, threads>>>(out, 0.999999f, 1e-6f);
+    launch(blocks, threads, out);
     cudaEventRecord(e1);
     e = cudaEventSynchronize(e1);
     float t = 0;
@@ -63,8 +80,38 @@ extern "C" int ppcb_fp32_peak(int device, int repeats, double* tflops, double* m
     ppcb_internal_set_error(cudaGetErrorString(e));
     return PPCB_ECUDA;
   }
-  const double flops = 2.0 * kChains * kIters * (double)blocks * threads;
+  *best_ms = best;
+  return PPCB_OK;
+}
+
+int grid_threads(int device) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return 0;
+  return p.multiProcessorCount * 4 * 256;
+}
+
+}  // namespace
+
+extern "C" int ppcb_fp32_peak(int device, int repeats, double* tflops, double* ms) {
+  if (!tflops || repeats <= 0) { ppcb_internal_set_error("ppcb_fp32_peak: bad argument"); return PPCB_EARG; }
+  double best = 0;
+  const int r = time_best(device, repeats, "ppcb_fp32_peak",
+                          [](int b, int t, float* out) { k_ffma<<<b, t>>>(out, 0.999999f, 1e-6f); }, &best);
+  if (r != PPCB_OK) return r;
+  const double flops = 2.0 * kChains * kIters * (double)grid_threads(device);
   *tflops = flops / (best * 1e-3) / 1e12;
+  if (ms) *ms = best;
+  return PPCB_OK;
+}
+
+extern "C" int ppcb_sfu_peak(int device, int repeats, double* tops, double* ms) {
+  if (!tops || repeats <= 0) { ppcb_internal_set_error("ppcb_sfu_peak: bad argument"); return PPCB_EARG; }
+  double best = 0;
+  const int r = time_best(device, repeats, "ppcb_sfu_peak",
+                          [](int b, int t, float* out) { k_mufu<<<b, t>>>(out, 1e-3f); }, &best);
+  if (r != PPCB_OK) return r;
+  const double ops = (double)kChains * kIters * (double)grid_threads(device);
+  *tops = ops / (best * 1e-3) / 1e12;
   if (ms) *ms = best;
   return PPCB_OK;
 }
