@@ -141,6 +141,38 @@ def cpu_reference_sample(photons_per_proc, procs, seed=0):
     return {"value": rate, "photons": photons, "seconds": secs}
 
 
+def cpu_par_sample(photons, seed=0, cascades=None):
+    """The reference's std::par build (oracle/_ref/ppc_par: par/ppc.cxx in CPU mode, OpenMP on
+    every host core) on cascades of the same workload (one per core by default, random
+    vertices and directions, `photons` in all), read as f2k records: photons/s over the run's
+    wall time less an empty run's (configuration loading)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ppc_par")
+    if not os.path.exists(exe):
+        return None
+    ice = os.path.join(ROOT, "ppc_b200", "data", "ice", "full")
+    rng = np.random.default_rng(seed)
+    n = cascades or (os.cpu_count() or 1)
+    E = photons / n * 25.0 / (2450.08 * 5.321 * 0.910 / 0.9216)
+    text = ""
+    for _ in range(n):
+        v = rng.uniform(-500, 500, 3)
+        th, ph = rng.uniform(0, 180), rng.uniform(0, 360)
+        text += f"TR 1 0 e {v[0]:.2f} {v[1]:.2f} {v[2]:.2f} {th:.3f} {ph:.3f} 0 {E:.3f} 0\n"
+    env = dict(os.environ, PPCTABLESDIR=ice + "/", OMP_NUM_THREADS=str(os.cpu_count() or 1))
+
+    def run(text):
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, "0"], input=text, env=env, capture_output=True, text=True, timeout=600)
+        return time.perf_counter() - t0, r
+
+    t_empty, _ = run("")
+    t, r = run(text)
+    if r.returncode != 0:
+        return None
+    n = sum(int(l.split()[1]) for l in r.stderr.splitlines() if l.startswith("photons:"))
+    return {"value": n / max(1e-9, t - t_empty), "photons": n, "seconds": t - t_empty}
+
+
 def _ref_harness_json(args, ice, exe="ref_harness_fm"):
     """One run of the reference harness (CPU build of the reference's own sources); its JSON
     line, or None when the harness is not built."""
@@ -675,27 +707,33 @@ def run_batched(args, local):
 
 
 def run_reference(args, rank, world):
+    """The reference's fastest CPU path on this host: its gpu/ CPU build (the reference's own
+    --fast-math flags) in one process per core.  Its std::par build on every core measured
+    slower on the same cascades (bench.py's cpu_baselines_other)."""
     if rank != 0:
         return
     procs = os.cpu_count() or 1
     per = args.ref_photons
+    par = False
     vals = []
     for s in range(args.warmup + args.steps):
-        r = cpu_reference_sample(per, procs, seed=s)
+        r = cpu_par_sample(per * procs, seed=s) if par else cpu_reference_sample(per, procs, seed=s)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not built"}))
             return
         if s >= args.warmup:
             vals.append(r)
     v = statistics.median([r["value"] for r in vals])
+    sample = (f"{per * procs} photons of {procs} cascades per step through the reference's std::par build on "
+              f"{procs} cores (oracle/_ref/ppc_par, OpenMP)" if par else
+              f"{per} photons x {procs} processes of the reference CPU build per step")
     line = {
         "impl": "reference", "metric": "photons/s", "value": v, "unit": "photons/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median([r["seconds"] for r in vals]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "full-detector EM cascade, 5160 DOMs, 171 layers, 1-d tilt, anisotropy, BFR",
                    "photons_per_step": per * procs, "l2": "n/a (host)"},
-        "cpu_baseline": {"value": v, "unit": "photons/s", "cores": procs, "kind": "reference",
-                         "sample": f"{per} photons x {procs} processes of the reference CPU build per step"},
+        "cpu_baseline": {"value": v, "unit": "photons/s", "cores": procs, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
@@ -873,12 +911,36 @@ def run_ours(args, rank, world, local):
     if single and not args.no_stages:
         line["stages"] = stages_sample(local)
     if single and not args.no_cpu_baseline:
-        r = cpu_reference_sample(args.ref_photons, os.cpu_count() or 1)
-        if r:
-            line["cpu_baseline"] = {"value": r["value"], "unit": "photons/s", "cores": os.cpu_count(),
-                                    "kind": "reference",
-                                    "sample": f"{args.ref_photons} photons x {os.cpu_count()} processes of the "
-                                              "reference CPU build (same cascade workload)"}
+        # the reference's CPU paths on the same workload: its std::par build on every core
+        # (the baseline, its fastest), its gpu/ CPU build in one process per core and on one
+        # thread
+        cores = os.cpu_count() or 1
+        rp = cpu_par_sample(cores * args.ref_photons)
+        r = cpu_reference_sample(args.ref_photons, cores)
+        r1 = cpu_reference_sample(args.ref_photons, 1, seed=1)
+        gpu_build = {"value": r["value"], "unit": "photons/s", "cores": cores, "kind": "reference",
+                     "sample": f"{args.ref_photons} photons x {cores} processes of the reference's gpu/ CPU "
+                               "build (same cascade workload)"} if r else None
+        par = {"value": rp["value"], "unit": "photons/s", "cores": cores, "kind": "reference",
+               "sample": f"{rp['photons']} photons of {cores} cascades through the reference's std::par build "
+                         "on every core (oracle/_ref/ppc_par, OpenMP)"} if rp else None
+        # the baseline is the faster of the two all-core paths
+        cands = [x for x in (gpu_build, par) if x]
+        others = {}
+        if cands:
+            best = max(cands, key=lambda x: x["value"])
+            line["cpu_baseline"] = best
+            if gpu_build and gpu_build is not best:
+                others["gpu_cpu_build_all_cores"] = gpu_build
+            if par and par is not best:
+                others["par_all_cores"] = par
+        if r1:
+            others["gpu_cpu_build_1_thread"] = {"value": r1["value"], "unit": "photons/s", "cores": 1,
+                                                "kind": "reference",
+                                                "sample": f"{args.ref_photons} photons, one process of the gpu/ "
+                                                          "CPU build (oracle/_ref/ref_harness_fm)"}
+        if others:
+            line["cpu_baselines_other"] = others
     print(json.dumps(line))
 
 
