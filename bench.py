@@ -714,19 +714,16 @@ def run_reference(args, rank, world):
         return
     procs = os.cpu_count() or 1
     per = args.ref_photons
-    par = False
     vals = []
     for s in range(args.warmup + args.steps):
-        r = cpu_par_sample(per * procs, seed=s) if par else cpu_reference_sample(per, procs, seed=s)
+        r = cpu_reference_sample(per, procs, seed=s)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not built"}))
             return
         if s >= args.warmup:
             vals.append(r)
     v = statistics.median([r["value"] for r in vals])
-    sample = (f"{per * procs} photons of {procs} cascades per step through the reference's std::par build on "
-              f"{procs} cores (oracle/_ref/ppc_par, OpenMP)" if par else
-              f"{per} photons x {procs} processes of the reference CPU build per step")
+    sample = f"{per} photons x {procs} processes of the reference's gpu/ CPU build per step"
     line = {
         "impl": "reference", "metric": "photons/s", "value": v, "unit": "photons/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median([r["seconds"] for r in vals]),
