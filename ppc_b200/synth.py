@@ -8,6 +8,7 @@ Workloads (sizes as used by the tests and the benchmark):
           -500 m, 100 layers of 10 m, b_e(400) ~ U[0.02,0.08]/m, a_dust(400) ~
           U[0.005,0.02]/m (numpy default_rng(1)), HG g=0.9, no tilt, no anisotropy, no
           birefringence; isotropic 405 nm point source at the origin.
+  small_xr1 `small` with DOMs at their true size (xR = 1 in cfg.txt instead of 5).
   full    86 strings (78 on a 125 m hexagonal lattice + 8 infill strings at ~70 m), 60
           DOMs each (5160), 171 layers of 10 m with smooth log-normal (sigma 0.3) b_e and
           a_dust profiles, 1-d tilt with a +-20 m sinusoidal dust-layer shift, absorption
@@ -108,8 +109,10 @@ _BFR = [0.0768, 5.4e5, 2.23, 0.00262, 0.0774, 1.55e6, 2.45, 0.00250, 0.00100, 0.
 
 
 def write(kind, path, count=131072, xR=5):
-    """Writes configuration `kind` (small | small_tilt | small_hole | full | full2d |
-    full_ng) into directory `path`."""
+    """Writes configuration `kind` (small | small_xr1 | small_tilt | small_hole | full |
+    full2d | full_ng) into directory `path`."""
+    if kind == "small_xr1":  # the 7-string detector with DOMs at their true size
+        kind, xR = "small", 1
     os.makedirs(path, exist_ok=True)
     shutil.copyfile(multipliers_file(count), os.path.join(path, "rnd.txt"))
     with open(os.path.join(path, "icemodel.par"), "w") as f:

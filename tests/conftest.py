@@ -39,6 +39,11 @@ def ice_full2d():
 
 
 @pytest.fixture(scope="session")
+def ice_small_xr1():
+    return _ice("small_xr1")
+
+
+@pytest.fixture(scope="session")
 def ice_full_ng():
     return _ice("full_ng")
 

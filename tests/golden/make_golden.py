@@ -42,8 +42,9 @@ RUNS = [
     ("small_tilt_led", "small_tilt", "flasher:1:30", 20000, 9, {"FWID": "9.7"}),
     ("small_hole_point", "small_hole", "point:0:0:0", 20000, 11, {"FWID": "-1", "WFLA": "405"}),
     ("full_ng_cascade", "full_ng", "cascade:-50:310:50:2000:0.3:0.4:0.8660254:11", 20000, 5, {}),
+    ("small_xr1_point", "small_xr1", "point:0:0:0", 200000, 13, {"FWID": "-1", "WFLA": "405"}),
 ]
-KINDS = ("small", "full", "full2d", "small_tilt", "small_hole", "full_ng")
+KINDS = ("small", "full", "full2d", "small_tilt", "small_hole", "full_ng", "small_xr1")
 
 # (case, configuration, source spec, photons, propagation seed, back-end seed): standard
 # sensors with cables and tilted axes; 24-PMT spheres, 2-PMT spheroids, shifting tubes

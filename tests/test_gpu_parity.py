@@ -214,6 +214,8 @@ def test_deterministic_photon_by_photon(ice_small):
 def _stat_sources():
     iso = T.bunch_led([0, 0, 0, 0], [0, 0, 1], 1, 0, 1, ka=-1, up=0, fldr=-1)
     yield "small_isotropic", "small", iso, 4_000_000, 200_000
+    # DOMs at their true size: 25 times fewer hits, and a photon ends on the DOM it hits
+    yield "small_xr1_isotropic", "small_xr1", iso, 40_000_000, 2_000_000
     # on the axis of the centre string: every photon starts inside its hole-ice column
     yield "small_hole_isotropic", "small_hole", iso, 4_000_000, 200_000
     yield "full2d_cascade", "full2d", T.bunch_particle([30, -20, 100, 0], [0.3, 0.4, np.sqrt(0.75)], 1, 0, -11, f=0.0,

@@ -27,7 +27,7 @@ def _product(ice, env, monkeypatch):
     return c
 
 
-@pytest.mark.parametrize("kind", ["small", "full", "full2d", "small_tilt", "small_hole", "full_ng"])
+@pytest.mark.parametrize("kind", ["small", "full", "full2d", "small_tilt", "small_hole", "full_ng", "small_xr1"])
 def test_product_tables_match_reference_golden(kind, request):
     """The loader's table image is bit-identical to the reference's (ini::set)."""
     ice = request.getfixturevalue("ice_" + kind)
@@ -53,9 +53,10 @@ def test_oracle_zshift_matches_reference_golden(kind, request):
     c.close()
 
 
-CASES = ["small_point", "full_cascade", "full2d_flasher", "small_tilt_led", "small_hole_point", "full_ng_cascade"]
+CASES = ["small_point", "full_cascade", "full2d_flasher", "small_tilt_led", "small_hole_point", "full_ng_cascade",
+         "small_xr1_point"]
 KIND = {"small_point": "small", "full_cascade": "full", "full2d_flasher": "full2d", "small_tilt_led": "small_tilt",
-        "small_hole_point": "small_hole", "full_ng_cascade": "full_ng"}
+        "small_hole_point": "small_hole", "full_ng_cascade": "full_ng", "small_xr1_point": "small_xr1"}
 
 
 @pytest.mark.parametrize("case", CASES)
