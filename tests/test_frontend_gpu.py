@@ -177,3 +177,8 @@ def test_f2k_event_device_front_end_matches_host_front_end(ctx):
     ctx.keep_raw(False)
     assert abs(host_ph - num) < 6 * math.sqrt(2 * num) + 0.03 * num, (host_ph, num)
     assert abs(len(hits_dev) - host_hits) < 6 * math.sqrt(2 * host_hits) + 0.03 * host_hits, (len(hits_dev), host_hits)
+
+
+def test_no_sources(ctx):
+    b, bstart, num = ctx.sources(np.zeros(0, T.SOURCE_DTYPE), seed=1)
+    assert len(b) == 0 and bstart.tolist() == [0] and num == 0

@@ -118,3 +118,15 @@ def test_time_shift_scan_finds_the_true_offset(runs):
         L.eval(raw, np.zeros(65), nsim=2.0)
     assert e.value.code == 7
     L.close()
+
+
+def test_no_simulated_hits(runs):
+    """Without simulated hits every block compares 0 against its observed charge."""
+    c, data, _ = runs
+    L = Likelihood(c, data)
+    out = L.eval(np.zeros(0, T.HIT_DTYPE), [0.0, 7.0], nsim=2.0)
+    ref, err = O.llh_fllh(data, np.zeros(0, O.LLHO_SIM_DTYPE), [0.0, 7.0], 2.0)
+    assert err == 0 and out[0] == out[1]
+    np.testing.assert_allclose(out, ref, rtol=1e-10)
+    assert len(c.accept(np.zeros(0, T.HIT_DTYPE))) == 0  # the back end on no hits
+    L.close()
