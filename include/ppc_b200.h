@@ -356,8 +356,8 @@ int ppcb_llh_eval(ppcb_llh* l, const ppcb_hit* hits, uint64_t n, uint32_t seed, 
 
 /* ---- measurement ----
  * No counterpart in the reference.  FP32 FMA throughput of `device` (TFLOP/s, best of
- * `repeats` launches of an FFMA loop over every SM): the denominator of the propagation
- * kernel's FP32 roofline. */
+ * `repeats` launches of an FFMA loop over every SM): the FP32 side of the propagation
+ * kernel's FP32/SFU issue roofline. */
 int ppcb_fp32_peak(int device, int repeats, double* tflops, double* ms);
 /* special-function-unit throughput (reciprocal square roots) of `device` in tera-operations
  * per second, measured the same way: the SFU side of the kernel's FP32/SFU issue roofline.
