@@ -656,7 +656,11 @@ def run_batched(args, local):
     oms = c.tables()["oms"]
     ev = W.batched_events(oms, n_events=args.events, seed=11)
     photons = int(ev["num"].sum())
-    b = Batch(c, max_events=args.events, max_bunches=args.events, hit_capacity=int(photons * 0.02) + 66 * args.events)
+    # the per-decade comparisons below reuse the batch: size it for the largest of the runs
+    dec_ev = {lo: W.batched_events(oms, n_events=512, lo=lo, hi=10 * lo, seed=int(lo)) for lo in (1e3, 1e4, 1e5, 1e6)}
+    most = max([photons] + [int(e["num"].sum()) for e in dec_ev.values()])
+    nmax = max(args.events, 512)
+    b = Batch(c, max_events=nmax, max_bunches=nmax, hit_capacity=int(most * 0.02) + 66 * nmax)
     tune = b.autotune(ev, args.events, sample_photons=50_000_000)
     for _ in range(max(1, args.warmup - 2)):
         b.run(ev, args.events, hits_per_photon=0.02)
@@ -680,8 +684,7 @@ def run_batched(args, local):
         "clocks": clocks,
     }
     decades = []
-    for lo in (1e3, 1e4, 1e5, 1e6):
-        ed = W.batched_events(oms, n_events=512, lo=lo, hi=10 * lo, seed=int(lo))
+    for lo, ed in dec_ev.items():
         b.run(ed, 512, hits_per_photon=0.02)  # capture for this size
         rr = [b.run(ed, 512, hits_per_photon=0.02) for _ in range(3)]
         t = sum(r["graph_ms"] for r in rr) / 1000.0
