@@ -108,10 +108,13 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, cons
   a.bunches = db.p; a.bstart = dbs.p; a.nb = nb; a.num = bs[nb];
   a.hits = dh.p; a.hcap = hit_cap; a.ctrl = dctrl.p; a.prov = dprov.p;
   check(cudaEventRecord(e0, st), "event");
-  // the recording kernel's shape: 256-thread blocks, all resident at once (a static photon
-  // order must not leave a second wave of blocks), and no more threads than streams
-  const int rec_blocks = std::min(g.prop.multiProcessorCount * propagate_max_blocks_per_sm(256), g.T / 256);
-  check(launch_propagate(a, LaunchShape{rec_blocks, 256}, st), "recording launch");
+  // the recording kernel's shape: the engine's block size (864 threads, one block per SM, or
+  // 256 threads, three per SM), all blocks resident at once (a static photon order must not
+  // leave a second wave of blocks), and no more threads than streams
+  const int tpb = threads_per_block == 864 ? 864 : 256;
+  const int per_sm = tpb == 864 ? 1 : propagate_max_blocks_per_sm(256);
+  const int rec_blocks = std::min(g.prop.multiProcessorCount * per_sm, g.T / tpb);
+  check(launch_propagate(a, LaunchShape{rec_blocks, tpb}, st), "recording launch");
   check(cudaEventRecord(e1, st), "event");
   ppcb_ctrl c;
   check(cudaMemcpyAsync(&c, dctrl.p, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H ctrl");

@@ -1217,8 +1217,11 @@ static cudaError_t launch_one(const KArgs& a, int blocks, cudaStream_t st) {
 template <bool REC, bool STREAMS>
 static cudaError_t launch_shape(const KArgs& a, LaunchShape sh, cudaStream_t st) {
   if constexpr (REC) {
-    if (sh.threads != 256) return cudaErrorInvalidConfiguration;
-    return launch_one<256, 3, true, STREAMS>(a, sh.blocks, st);
+    switch (sh.threads) {
+      case 256: return launch_one<256, 3, true, STREAMS>(a, sh.blocks, st);
+      case 864: return launch_one<864, 1, true, STREAMS>(a, sh.blocks, st);
+      default: return cudaErrorInvalidConfiguration;
+    }
   } else {
     switch (sh.threads) {
       case 256: return launch_one<256, 3, false, STREAMS>(a, sh.blocks, st);
