@@ -223,15 +223,20 @@ int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t e
  * No counterpart in the reference.  For callers that may not allocate device memory while
  * they run: frameworks that reserve the GPU's memory for their own pool at start-up, and
  * steady-state loops where a cudaMalloc/cudaFree would synchronise the device.  Same
- * launch as ppcb_propagate_device, but its scratch (photon work counter, hit counter and
- * per-bunch photon offsets) is a static device array of fixed size inside the library:
- * at most PPCB_NOALLOC_MAX_BUNCHES bunches per call (larger lists are rejected with
- * PPCB_EARG).  The caller passes the bunches, the hit buffer and `nhits`, a device
- * pointer that receives the number of hits produced (only the first hcap are stored).
- * The call allocates nothing; the context's tables come from an earlier ppcb_ini.
- * The first call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls on a device share the one array: calls whose work
- * overlaps on the GPU race, so order them (one stream, or events). */
+ * launch as ppcb_propagate_device, but its scratch (photon work counter, hit counter,
+ * launch sizes and per-bunch photon offsets) is a static device array of fixed size inside
+ * the library: at most PPCB_NOALLOC_MAX_BUNCHES bunches per call (larger lists are rejected
+ * with PPCB_EARG).  The caller passes the bunches (device memory), the hit buffer and
+ * `nhits`, a device pointer that receives the number of hits produced; when that number
+ * exceeds hcap only the first hcap records are stored.  `num` is the sum of
+ * bunches[k].num: a smaller value propagates the first `num` photons, a larger one is
+ * clamped to the sum on the device.  The call allocates nothing; the context's tables come
+ * from an earlier ppcb_ini.  The caller's current device is left as it was.
+ * Each call looks up the array's device address with the device current (a host-side
+ * lookup, no allocation); the first call on a device may load the library's device code,
+ * so make that first call before any stream capture.  All calls on a device share the one
+ * array and it keeps the last call's contents (each call clears its counters first): calls
+ * whose work overlaps on the GPU race, so order them (one stream, or events). */
 #define PPCB_NOALLOC_MAX_BUNCHES 65536
 int ppcb_propagate_noalloc(ppcb_ctx* c, int device, const ppcb_bunch* bunches, int32_t nb, uint64_t num,
                            ppcb_hit* hits, uint64_t hcap, uint64_t* nhits, void* stream);

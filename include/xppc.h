@@ -4,7 +4,7 @@
 // llh/ppc.h:1-113 and defines it in gpu/ppc.cu + gpu/f2k.cxx under -DXLIB).  Names,
 // signatures, record layouts and ordering operators are kept identical so that a
 // program compiled against the reference header links against libxppc.so from this
-// package unchanged (see INTEGRATION.md).  Each declaration cites the reference
+// package unchanged.  Each declaration cites the reference
 // definition it replaces.
 #ifndef PPC_B200_XPPC_H
 #define PPC_B200_XPPC_H

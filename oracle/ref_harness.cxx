@@ -29,7 +29,9 @@
 //      times the reference's own front end (addp: yield, poidev, addh; gpu/f2k.cxx:17-167,
 //      377-504) over (f32 x, y, z, t, E, dr, i32 type) per source; the bunches are dropped
 //      before a batch fills, so no propagation runs.  Prints photons and seconds.
-//   ref_harness run <spec> <photons> <seed> <out-prefix> [nodump]
+//   ref_harness run <spec> <photons> <seed> <out-prefix> [nodump | hits]
+//      writes <out-prefix>.hits, .pbuf and .bunch; "nodump" writes nothing (timing),
+//      "hits" only the kernel-level hit records (high-statistics runs)
 //      spec = "flasher:<str>:<om>" | "cascade:<x>:<y>:<z>:<E>:<nx>:<ny>:<nz>:<type>"
 //           | "point:<x>:<y>:<z>"   (isotropic point source, FWID=-1 style, at x,y,z)
 #include "ppc.cu"
@@ -242,7 +244,9 @@ int main(int argc, char** argv) {
     unsigned long long total = strtoull(argv[3], 0, 10);
     unsigned int seedv = strtoul(argv[4], 0, 10);
     std::string outp = argv[5];
-    bool dump = !(argc >= 7 && std::string(argv[6]) == "nodump");
+    const std::string opt = argc >= 7 ? argv[6] : "";
+    const bool dump = opt != "nodump" && opt != "hits";
+    const bool keep_hits = opt != "nodump";
     initialize();
     sv = seedv;      // DTMN leaves sv at 0; the caller picks the stream start
     choose(0);
@@ -281,14 +285,17 @@ int main(int argc, char** argv) {
       if (dump) bunches.push_back(p);
       auto t0 = std::chrono::steady_clock::now();
       produced += launch(num, hits, dump ? &bufs : nullptr);
+      if (!keep_hits) hits.clear();
       secs += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       done += num;
     }
-    if (dump) {
+    if (keep_hits) {
       FILE* f = xopen((outp + ".hits").c_str(), "wb");
       fwrite(hits.data(), sizeof(hit), hits.size(), f);
       fclose(f);
-      f = xopen((outp + ".pbuf").c_str(), "wb");
+    }
+    if (dump) {
+      FILE* f = xopen((outp + ".pbuf").c_str(), "wb");
       fwrite(bufs.data(), sizeof(pbuf), bufs.size(), f);
       fclose(f);
       f = xopen((outp + ".bunch").c_str(), "wb");

@@ -12,7 +12,7 @@ oracle/_ref/ref_harness) on the synthetic configurations of ppc_b200/synth.py an
                         kernel-level hits of a propagation: its input hits, host seed and the
                         hit map it fills
 
-Needs /root/reference (run in the build container):
+Needs the reference sources where oracle/Makefile's REF points (run in the build container):
     python tests/golden/make_golden.py [names...]   (configurations / cases; default all)
 """
 import hashlib

@@ -14,7 +14,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "libppc_oracle.so")
 REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 REF_PPC = os.path.join(ROOT, "oracle", "_ref", "ppc")
-REFERENCE = "/root/reference"
+
+
+def _reference_dir():
+    """The reference source tree as oracle/Makefile names it (its REF variable)."""
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "refdir"], capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
+REFERENCE = _reference_dir()
 
 
 class Tables(C.Structure):

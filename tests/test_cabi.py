@@ -77,8 +77,9 @@ int main(int argc, char** argv) {
 @pytest.mark.parametrize("header", ["ours", "reference"])
 def test_program_written_against_api_links(header, tmp_path):
     if header == "reference":
-        h = "/root/reference/llh/ppc.h"
-        if not os.path.exists(h):
+        import oracle_util as O
+        h = os.path.join(O.REFERENCE, "llh", "ppc.h")
+        if not O.REFERENCE or not os.path.exists(h):
             pytest.skip("reference header not present")
         src = LLH_LIKE.replace("HEADER", '"' + h + '"')
     else:

@@ -65,7 +65,7 @@ int main() {
   xppc::ini();
   xppc::flset(21, 30);
   xppc::sett(0, 0, 1, std::make_pair(3, 9ULL), 0);
-  xppc::flone(4000000);
+  xppc::flone(40000000);
   xppc::eout();
   size_t n = 0;
   for (xppc::outz::const_iterator i = xppc::hitz.begin(); i != xppc::hitz.end(); ++i) n += i->second.size();
@@ -79,7 +79,7 @@ int main() {
 """
 
 
-def test_program_linked_against_libxppc_runs(ice_full, tmp_path):
+def test_program_linked_against_libxppc_runs(ice_full, tmp_path, monkeypatch):
     lib = os.path.join(ROOT, "ppc_b200", "lib")
     src = tmp_path / "llh_like.cxx"
     src.write_text(LLH_LIKE)
@@ -91,7 +91,23 @@ def test_program_linked_against_libxppc_runs(ice_full, tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, (r.stdout[-500:], r.stderr[-2000:])
     n = int([l for l in r.stdout.splitlines() if l.startswith("hitz")][0].split()[1])
-    assert n > 100
+    # the same flasher through the Python path of the same library: the two counts are
+    # independent Poisson-like samples of one mean, so they agree within 5 sigma
+    monkeypatch.setenv("FLDR", "3960")
+    monkeypatch.setenv("ELEV", "30")
+    c = PPC()
+    c.initialize(1.0, ice_full)
+    c.choose(0)
+    c.ini()
+    c.flset(21, 30)
+    c.sett(0.0, 0.0, 1.0, (3, 9), 0)
+    c.flone(40_000_000)
+    c.eout()
+    m = len(c.hitz())
+    c.efin()
+    c.close()
+    assert m > 300, m  # the mean is about 1000 hits: this floor is more than 20 sigma below it
+    assert abs(n - m) < 5 * np.sqrt(n + m), (n, m)
 
 
 def test_device_back_end_matches_host_back_end(ice_full2d, monkeypatch):
