@@ -156,6 +156,11 @@ int ppcb_generate_device(ppcb_ctx* c, int device, const ppcb_bunch* bunches, con
  * tilt shift, layer thickness (gpu/pro.cu:168-264, :507-515, :580-594, :623-626). */
 int ppcb_index_probe_device(ppcb_ctx* c, int device, const void* pos, int32_t n, int32_t* out_i, float* out_f,
                             void* stream);
+/* The kernel's string-proximity pre-test of the DOM search, on the host (same code): for
+ * segments pos[2k] = (x,y,z,t), pos[2k+1] = (nx,ny,nz,length), out[k] = 1 when the
+ * segment may reach a string's cylinder (the reference's search, gpu/pro.cu:577-672, then
+ * runs), 0 when that search would find nothing.  Needs ppcb_initialize only. */
+int ppcb_string_grid_probe(ppcb_ctx* c, const void* pos, int32_t n, int32_t* out);
 
 /* ---- batched events ----
  * No counterpart in the reference, which propagates one source per eout()

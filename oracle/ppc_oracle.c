@@ -730,3 +730,45 @@ void ppco_index_probe(const ppco_tables* t, const float* pos, int n, int32_t* oi
     of[2 * k + 1] = dz;
   }
 }
+
+/* The string loop of the DOM search (gpu/pro.cu:577-672) for one segment per row of `pos`
+ * (x, y, z, t, nx, ny, nz, length): out[2k] counts the strings of the visited search cells
+ * whose cylinder test passes (gpu/pro.cu:601-607), out[2k+1] those whose hole-ice column
+ * test passes (gpu/pro.cu:655-660, taken as if hole ice were on at every time). */
+void ppco_string_pass(const ppco_tables* t, const float* pos, int n, int32_t* out) {
+  const ppcb_params* e = t->p;
+  for (int k = 0; k < n; k++) {
+    const float* r = pos + 8 * k;
+    const float* d = r + 4;
+    const float sca = d[3];
+    int pass = 0, hole = 0;
+    int xlx, xhx, xly, xhy;
+    cell_range(e, r[0], r[1], r[0] + sca * d[0], r[1] + sca * d[1], &xlx, &xhx, &xly, &xhy);
+    for (int i = xlx, j = xly; i <= xhx && j <= xhy; (++j <= xhy) ? 0 : (j = xly, i++)) {
+      for (unsigned short q = t->is[i * PPCB_CY + j]; q != 0x8000;) {
+        unsigned short m = t->ls[q];
+        const ppcb_line* sl = &t->sc[m & 0x7fff];
+        q = (m & 0x8000) ? 0x8000 : q + 1;
+        float b = 0, c = 0, dr;
+        dr = sl->x - r[0]; b += d[0] * dr; c += dr * dr;
+        dr = sl->y - r[1]; b += d[1] * dr; c += dr * dr;
+        float np = 1 - d[2] * d[2];
+        float D = b * b - (c - sl->r * sl->r) * np;
+        if (D >= 0) {
+          D = sqrtf(D);
+          if (b + D >= 0 && b - D <= sca * np) pass++;
+        }
+        if (e->hr > 0) {
+          float DH = b * b - (c - e->hr2) * np;
+          if (DH > 0) {
+            DH = sqrtf(DH);
+            if (b + DH >= 0 && b - DH <= sca * np) hole++;
+          }
+        }
+      }
+    }
+    out[2 * k] = pass;
+    out[2 * k + 1] = hole;
+  }
+}
+

@@ -67,6 +67,7 @@ uint64_t ppco_run_fused(const ppco_tables* t, const ppcb_bunch* b, int nb, uint6
 /* Index helpers at points (the product's ppcb_index_probe_device counterpart):
  * pos[8k..] = x,y,z,t, nx,ny,nz,length; out as there. */
 void ppco_index_probe(const ppco_tables* t, const float* pos, int n, int32_t* out_i, float* out_f);
+void ppco_string_pass(const ppco_tables* t, const float* pos, int n, int32_t* out);
 
 #ifdef __cplusplus
 }

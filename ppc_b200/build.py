@@ -43,7 +43,7 @@ CU_FAST_MATH = ["--use_fast_math"]
 CU_EXACT = {"frontend.cu"}
 CLI = ["ppc_cli.cpp"]
 HEADERS = ["ppcb_types.h", "config.h", "engine.h", "propagate.cuh", "session.h", "ctx.h", "tilt.h", "batch.h",
-           "backend.cuh", "llh.h"]
+           "backend.cuh", "llh.h", "strgrid.h"]
 
 
 def _newer(target, deps):

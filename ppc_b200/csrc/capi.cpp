@@ -394,6 +394,24 @@ int ppcb_index_probe_device(ppcb_ctx* c, int device, const void* pos, int32_t n,
   });
 }
 
+int ppcb_string_grid_probe(ppcb_ctx* c, const void* pos, int32_t n, int32_t* out) {
+  CTX_OR_FAIL(c);
+  if (n < 0 || (n > 0 && (!pos || !out))) { g_err = "bad arguments"; return PPCB_EARG; }
+  return guard([&] {
+    const ppcb::Config& f = c->s.eng.cfg;
+    struct HostTab {
+      const ppcb::Config& f;
+      uint32_t cell(int k) const { return f.sg_cells[k]; }
+      const ppcb::StrGroup& group(int m) const { return f.sg_groups[m]; }
+    } t{f};
+    const float* p = static_cast<const float*>(pos);
+    for (int32_t k = 0; k < n; k++) {
+      const float* r = p + 8 * k;
+      out[k] = ppcb::sg_may_reach(f.sg, t, r[0], r[1], r[4], r[5], r[6], r[7]) ? 1 : 0;
+    }
+  });
+}
+
 }  // extern "C"
 
 void ppcb_internal_set_error(const std::string& msg) { g_err = msg; }

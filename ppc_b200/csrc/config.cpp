@@ -706,6 +706,8 @@ void Config::load(const std::string& tables_dir) {
       }
   }
 
+  build_strgrid();
+
   // ice layer tilt, gpu/ini.cxx:1178-1319
   p.tmod = 0;
   lr.assign(PPCB_LMAX, 0.f);
@@ -1054,6 +1056,73 @@ void Config::load(const std::string& tables_dir) {
     wmeta[n].wvl = n; wmeta[n].ocm = ng / c;
     wmeta[n].coschr = 1 / npv; wmeta[n].sinchr = sqrt(1 - wmeta[n].coschr * wmeta[n].coschr);
   }
+}
+
+// String-proximity table (strgrid.h).  Lines on the same axis form a group (its disc covers
+// theirs, widened by kReachPad); a square grid over the groups' footprint plus a
+// 64 m margin, with cells as small as kSgMaxCells allows (from 8 m up), stores per cell the
+// nearest group and a lower bound on the distance from the cell to every other group's
+// widened disc (exact on the cell square, rounded down to kSgClearUnit).  Not part of the
+// reference's tables: it only decides when the reference's DOM search can be skipped.
+void Config::build_strgrid() {
+  sg = StrGridParams{};
+  sg_groups.clear();
+  sg_cells.clear();
+  if (p.nstr <= 0) return;
+  // lines whose axes are within a metre of a group's axis join it (a string split into
+  // lines has the same axis up to rounding); the group's disc covers each line's disc
+  for (int m = 0; m < p.nstr; m++) {
+    bool merged = false;
+    for (auto& g : sg_groups) {
+      const double d = std::hypot((double)sc[m].x - g.x, (double)sc[m].y - g.y);
+      if (d < 1) {
+        g.rw = std::max(g.rw, (float)(d + sc[m].r + kReachPad) * (1 + 1e-6f));
+        merged = true;
+        break;
+      }
+    }
+    if (!merged) sg_groups.push_back(StrGroup{sc[m].x, sc[m].y, sc[m].r + kReachPad, 0});
+  }
+  if (sg_groups.size() >= kSgNone) throw Error("string-proximity table: too many string axes");
+  const double margin = 64;
+  double x0 = 1e30, x1 = -1e30, y0 = 1e30, y1 = -1e30;
+  for (auto& g : sg_groups) {
+    x0 = std::min(x0, (double)g.x - g.rw); x1 = std::max(x1, (double)g.x + g.rw);
+    y0 = std::min(y0, (double)g.y - g.rw); y1 = std::max(y1, (double)g.y + g.rw);
+  }
+  double cell = 8;
+  int nx = 0, ny = 0;
+  for (;;) {
+    nx = (int)std::ceil((x1 - x0 + 2 * margin) / cell);
+    ny = (int)std::ceil((y1 - y0 + 2 * margin) / cell);
+    if ((long)nx * ny <= kSgMaxCells) break;
+    cell *= 1.25;
+  }
+  sg.ox = (float)(x0 - margin);
+  sg.oy = (float)(y0 - margin);
+  sg.inv = (float)(1 / cell);
+  sg.margin = (float)margin;
+  sg.nx = nx; sg.ny = ny; sg.on = 1;
+  sg_cells.assign((size_t)nx * ny, 0);
+  const int ng = (int)sg_groups.size();
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      // the cell as the device indexes it, widened by a micrometre on each side
+      const double xa = sg.ox + i * cell - 1e-6, xb = sg.ox + (i + 1) * cell + 1e-6;
+      const double ya = sg.oy + j * cell - 1e-6, yb = sg.oy + (j + 1) * cell + 1e-6;
+      int best = -1;
+      double d1 = 1e30, d2 = 1e30;  // nearest and second-nearest disc distance
+      for (int k = 0; k < ng; k++) {
+        const double gx = sg_groups[k].x, gy = sg_groups[k].y;
+        const double qx = gx - std::min(std::max(gx, xa), xb), qy = gy - std::min(std::max(gy, ya), yb);
+        const double d = std::max(0.0, std::sqrt(qx * qx + qy * qy) - (double)sg_groups[k].rw);
+        if (d < d1) { d2 = d1; d1 = d; best = k; }
+        else if (d < d2) d2 = d;
+      }
+      const double q = std::floor(d2 / kSgClearUnit);
+      const unsigned int clear = q > 255 ? 255u : (unsigned int)q;
+      sg_cells[(size_t)j * nx + i] = (uint16_t)((clear << 8) | (unsigned int)(best < 0 ? kSgNone : best));
+    }
 }
 
 }  // namespace ppcb

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "ppcb_types.h"
+#include "strgrid.h"
 
 namespace ppcb {
 
@@ -124,6 +125,10 @@ class Config {
   std::vector<uint32_t> rm;                // [rsize]
   std::vector<float> bfrt;                 // [(BFR_TAB+1)*4] birefringence functions of v = sqrt(1-|cos|)
   std::vector<float> wgrad;                // [WNUM*2] d sca/d be, d abs/d ba per wavelength bin
+  // string-proximity table over sc (strgrid.h): geometry, groups, cell entries [nx*ny]
+  StrGridParams sg{};
+  std::vector<StrGroup> sg_groups;
+  std::vector<uint16_t> sg_cells;
 
   // ---- host-side tables ----
   std::vector<OMName> names;               // [gsize]
@@ -154,6 +159,7 @@ class Config {
 
  private:
   void fill_ice(int n, float wva);
+  void build_strgrid();
   unsigned short sname(int n);
   std::map<int, unsigned short> sname_overflow_;
   unsigned short sname_next_ = 86 + 10 + 1;

@@ -137,6 +137,12 @@ void Engine::ini() {
     upload(g.mcol, cfg.mcol.data(), PPCB_CTX * PPCB_CTY, "mcol");
     g.bfrt = dalloc<float4>(PPCB_BFR_TAB + 1, "bfrt");
     upload(g.bfrt, (const float4*)cfg.bfrt.data(), PPCB_BFR_TAB + 1, "bfrt");
+    if (cfg.sg.on) {
+      g.sg_groups = dalloc<StrGroup>(cfg.sg_groups.size(), "sg_groups");
+      upload(g.sg_groups, cfg.sg_groups.data(), cfg.sg_groups.size(), "sg_groups");
+      g.sg_cells = dalloc<uint16_t>(cfg.sg_cells.size(), "sg_cells");
+      upload(g.sg_cells, cfg.sg_cells.data(), cfg.sg_cells.size(), "sg_cells");
+    }
     g.rs = dalloc<uint64_t>(g.T, "rs");
     g.rm = dalloc<uint32_t>(g.T, "rm");
     upload(g.rm, cfg.rm.data(), g.T, "rm");
@@ -180,10 +186,11 @@ void Engine::free_device(DeviceCtx& g) {
   g.front.reset();
   if (g.st) cudaStreamSynchronize(g.st);
   if (g.cp) cudaStreamSynchronize(g.cp);
-  void* ptrs[] = {g.absca, g.wmeta, g.lp, g.oms, g.az, g.sc, g.lr, g.ls, g.is, g.mcol, g.bfrt, g.rs, g.rm};
+  void* ptrs[] = {g.absca, g.wmeta, g.lp, g.oms, g.az, g.sc, g.lr, g.ls, g.is, g.mcol, g.bfrt, g.sg_groups, g.sg_cells,
+                  g.rs, g.rm};
   for (void* p : ptrs) if (p) cudaFree(p);
   g.absca = nullptr; g.wmeta = nullptr; g.lp = nullptr; g.oms = nullptr; g.az = nullptr; g.sc = nullptr;
-  g.bfrt = nullptr;
+  g.bfrt = nullptr; g.sg_groups = nullptr; g.sg_cells = nullptr;
   g.lr = nullptr; g.ls = nullptr; g.is = nullptr; g.mcol = nullptr; g.rs = nullptr; g.rm = nullptr;
   for (auto& S : g.slot) {
     if (S.bunches) cudaFree(S.bunches);
@@ -221,6 +228,8 @@ KArgs Engine::args_for(int d) const {
   a.p = cfg.p;
   a.absca = g.absca; a.wmeta = g.wmeta; a.lp = g.lp; a.oms = g.oms; a.az = g.az; a.sc = g.sc;
   a.lr = g.lr; a.ls = g.ls; a.is = g.is; a.mcol = g.mcol; a.bfrt = g.bfrt;
+  a.sg = cfg.sg; a.sg_groups = g.sg_groups; a.sg_ngroups = (int)cfg.sg_groups.size(); a.sg_cells = g.sg_cells;
+  if (!a.sg_cells) a.sg.on = 0;
   a.rs = g.rs; a.rm = g.rm;
   a.deterministic = deterministic;
   a.seed = sv;

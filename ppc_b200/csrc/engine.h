@@ -48,6 +48,8 @@ struct DeviceCtx {
   uint16_t* is = nullptr;
   int8_t* mcol = nullptr;
   float4* bfrt = nullptr;
+  StrGroup* sg_groups = nullptr;   // string-proximity table (strgrid.h)
+  uint16_t* sg_cells = nullptr;
   uint64_t* rs = nullptr;
   uint32_t* rm = nullptr;
   struct Slot {

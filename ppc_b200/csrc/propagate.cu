@@ -46,6 +46,7 @@ struct SmemTables {
   uint16_t is[PPCB_CX * PPCB_CY];
   int8_t mcol[PPCB_CTX * PPCB_CTY];
   float4 bfrt[PPCB_BFR_TAB + 1];  // birefringence angular functions (sx, sy, mx, -)
+  StrGroup sgg[PPCB_NSTR];        // string-proximity table: string axes (strgrid.h)
 };
 
 // ---------------------------------------------------------------- IEEE helpers
@@ -593,10 +594,98 @@ __device__ __noinline__ void record_nan_step(const KArgs& a) {
   if (k < 4) { unsigned int sm; asm volatile("mov.u32 %0, %%smid;" : "=r"(sm)); a.ctrl->bad_sm[k] = sm; }
 }
 
+// String-proximity table as the kernel reads it: cell entries in dynamic shared memory,
+// string axes in the static tables.
+struct SgTab {
+  const SmemTables& S;
+  const uint16_t* cells;
+  __device__ __forceinline__ uint32_t cell(int k) const { return cells[k]; }
+  __device__ __forceinline__ const StrGroup& group(int m) const { return S.sgg[m]; }
+};
+
+// Result of the DOM search: the hit DOM (or -1) and its distance, the hole-ice column
+// entry and exit, and sqd of the last DOM whose quadratic had a root (gpu/pro.cu:644).
+struct Found {
+  int om;
+  float del, hi, hf, sqd;
+};
+
+// gpu/pro.cu:577-672: the DOM search through the search-cell grid, in the reference's
+// order (cells, then the strings of each cell, then the DOM window of each string).  It
+// runs only for the steps the string-proximity table cannot rule out.  Inlined: as a call
+// it would make the step save and restore its live registers around the call site.
+__device__ __forceinline__ Found dom_search(const KArgs& a, const SmemTables& S, float4 r, float4 n, float sca, int old,
+                                         int ofla) {
+  const ppcb_params& e = a.p;
+  int om = -1;
+  float del = sca, hi = sca, hf = 0, sqd = 0;
+  {  // DOM search, gpu/pro.cu:577-672
+    int xlx, xhx, xly, xhy;
+    cell_range(e, r.x, r.y, fa(r.x, fm(sca, n.x)), fa(r.y, fm(sca, n.y)), xlx, xhx, xly, xhy);
+    const bool hole_on = e.hr > 0 && (e.hifl == 0 || (e.hifl < 0 && r.w < -e.hifl) || (e.hifl > 0 && r.w > e.hifl));
+    for (int i = xlx, j = xly; i <= xhx && j <= xhy; (++j <= xhy) ? 0 : (j = xly, i++)) {
+      for (unsigned int k = S.is[i * PPCB_CY + j]; k != 0x8000;) {
+        unsigned int m = S.ls[k];
+        const ppcb_line& sl = S.sc[m & 0x7fff];
+        k = (m & 0x8000) ? 0x8000 : k + 1;
+        float b = 0, c = 0, dr;
+        dr = sl.x - r.x; b += n.x * dr; c += dr * dr;
+        dr = sl.y - r.y; b += n.y * dr; c += dr * dr;
+        float np = 1 - n.z * n.z;
+        float D = b * b - (c - sl.r * sl.r) * np;
+        if (D >= 0) {
+          D = sqrtf(D);
+          float h1 = b - D, h2 = b + D;
+          if (h2 >= 0 && h1 <= sca * np) {
+            if (np > XXX) {
+              h1 /= np; h2 /= np;
+              if (h1 < 0) h1 = 0;
+              if (h2 > sca) h2 = sca;
+            } else { h1 = 0; h2 = sca; }
+            h1 = r.z + n.z * h1; h2 = r.z + n.z * h2;
+            float zl, zh;
+            if (n.z > 0) { zl = h1; zh = h2; }
+            else { zl = h2; zh = h1; }
+            int n1, n2;
+            dom_window(sl, zl, zh, n1, n2);
+            for (int l = n1; l <= n2; l++) if (l != old) {
+              const ppcb_dom dom = a.oms[l];
+              float aa = 0, bb = 0, cc = 0, dd;
+              float fq = dom.F > 0 ? (1 / dom.F) * (1 / dom.F) : 0;
+              dd = dom.r[0] - r.x; aa += n.x * n.x; bb += n.x * dd; cc += dd * dd;
+              dd = dom.r[1] - r.y; aa += n.y * n.y; bb += n.y * dd; cc += dd * dd;
+              dd = dom.r[2] - r.z; aa += fq * n.z * n.z; bb += fq * n.z * dd; cc += fq * dd * dd;
+              if (aa > 0) {
+                bb /= aa;
+                float xR = (l == ofla ? 1 : e.xR);
+                float DD = bb * bb - (cc - (xR * dom.R) * (xR * dom.R)) / aa;
+                if (DD >= 0) {
+                  sqd = sqrtf(DD);
+                  float h = bb - sqd;
+                  if (dom.F > 0 || fabsf(dd - n.z * h) < -xR * dom.F * dom.R) {
+                    sqd /= xR; h = bb - sqd;
+                    if (h > 0 && h <= del) { om = l; del = h; }
+                  }
+                }
+              }
+            }
+          }
+        }
+        if (hole_on) {  // hole-ice column around the string
+          const float2 h = hole_column(e, b, c, np, sca, hi, hf);
+          hi = h.x; hf = h.y;
+        }
+      }
+    }
+  }
+
+  return Found{om, del, hi, hf, sqd};
+}
+
 // gpu/pro.cu:499-888: one propagation step (one scattering segment).  Returns with
 // ph.TOT == 0 once the photon is absorbed or registered.
 template <class HOOK>
-__device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon& ph, Rng& s,
+__device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const uint16_t* sgc, Photon& ph, Rng& s,
                                      unsigned int& nan_steps, HOOK& hk) {
   const ppcb_params& e = a.p;
   const float2* __restrict__ wz = a.absca + (size_t)ph.wl * e.size;
@@ -664,64 +753,12 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, Photon
   om = -1;
   float del = sca;
   float hi = sca, hf = 0;
-  {  // DOM search, gpu/pro.cu:577-672
-    int xlx, xhx, xly, xhy;
-    cell_range(e, r.x, r.y, fa(r.x, fm(sca, n.x)), fa(r.y, fm(sca, n.y)), xlx, xhx, xly, xhy);
-    const bool hole_on = e.hr > 0 && (e.hifl == 0 || (e.hifl < 0 && r.w < -e.hifl) || (e.hifl > 0 && r.w > e.hifl));
-    for (int i = xlx, j = xly; i <= xhx && j <= xhy; (++j <= xhy) ? 0 : (j = xly, i++)) {
-      for (unsigned int k = S.is[i * PPCB_CY + j]; k != 0x8000;) {
-        unsigned int m = S.ls[k];
-        const ppcb_line& sl = S.sc[m & 0x7fff];
-        k = (m & 0x8000) ? 0x8000 : k + 1;
-        float b = 0, c = 0, dr;
-        dr = sl.x - r.x; b += n.x * dr; c += dr * dr;
-        dr = sl.y - r.y; b += n.y * dr; c += dr * dr;
-        float np = 1 - n.z * n.z;
-        float D = b * b - (c - sl.r * sl.r) * np;
-        if (D >= 0) {
-          D = sqrtf(D);
-          float h1 = b - D, h2 = b + D;
-          if (h2 >= 0 && h1 <= sca * np) {
-            if (np > XXX) {
-              h1 /= np; h2 /= np;
-              if (h1 < 0) h1 = 0;
-              if (h2 > sca) h2 = sca;
-            } else { h1 = 0; h2 = sca; }
-            h1 = r.z + n.z * h1; h2 = r.z + n.z * h2;
-            float zl, zh;
-            if (n.z > 0) { zl = h1; zh = h2; }
-            else { zl = h2; zh = h1; }
-            int n1, n2;
-            dom_window(sl, zl, zh, n1, n2);
-            for (int l = n1; l <= n2; l++) if (l != old) {
-              const ppcb_dom dom = a.oms[l];
-              float aa = 0, bb = 0, cc = 0, dd;
-              float fq = dom.F > 0 ? (1 / dom.F) * (1 / dom.F) : 0;
-              dd = dom.r[0] - r.x; aa += n.x * n.x; bb += n.x * dd; cc += dd * dd;
-              dd = dom.r[1] - r.y; aa += n.y * n.y; bb += n.y * dd; cc += dd * dd;
-              dd = dom.r[2] - r.z; aa += fq * n.z * n.z; bb += fq * n.z * dd; cc += fq * dd * dd;
-              if (aa > 0) {
-                bb /= aa;
-                float xR = (l == ph.ofla ? 1 : e.xR);
-                float DD = bb * bb - (cc - (xR * dom.R) * (xR * dom.R)) / aa;
-                if (DD >= 0) {
-                  sqd = sqrtf(DD);
-                  float h = bb - sqd;
-                  if (dom.F > 0 || fabsf(dd - n.z * h) < -xR * dom.F * dom.R) {
-                    sqd /= xR; h = bb - sqd;
-                    if (h > 0 && h <= del) { om = l; del = h; }
-                  }
-                }
-              }
-            }
-          }
-        }
-        if (hole_on) {  // hole-ice column around the string
-          const float2 h = hole_column(e, b, c, np, sca, hi, hf);
-          hi = h.x; hf = h.y;
-        }
-      }
-    }
+  // DOM search, gpu/pro.cu:577-672: only for the steps that may reach a string's cylinder
+  // (strgrid.h; on the full detector about 0.2% of them); for the others it would find
+  // nothing and leave om, del, hi, hf and sqd as they are
+  if (sg_may_reach(a.sg, SgTab{S, sgc}, r.x, r.y, n.x, n.y, n.z, sca)) {
+    const Found f = dom_search(a, S, r, n, sca, old, ph.ofla);
+    om = f.om; del = f.del; hi = f.hi; hf = f.hf; sqd = f.sqd;
   }
 
   float fin = fminf(del, hi);
@@ -874,6 +911,17 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
   for (int i = t; i < PPCB_CX * PPCB_CY; i += nt) S.is[i] = a.is[i];
   for (int i = t; i < PPCB_CTX * PPCB_CTY; i += nt) S.mcol[i] = a.mcol[i];
   for (int i = t; i <= PPCB_BFR_TAB; i += nt) S.bfrt[i] = a.bfrt[i];
+  for (int i = t; i < a.sg_ngroups; i += nt) S.sgg[i] = a.sg_groups[i];
+  __syncthreads();
+}
+
+// The string-proximity cell entries into (dynamic) shared memory; bytes they take there.
+__host__ __device__ __forceinline__ size_t sg_cells_bytes(const KArgs& a) {
+  return a.sg.on ? (((size_t)a.sg.nx * a.sg.ny * sizeof(uint16_t) + 15) & ~(size_t)15) : 0;
+}
+__device__ __forceinline__ void load_cells(const KArgs& a, uint16_t* cells) {
+  const int n = a.sg.on ? a.sg.nx * a.sg.ny : 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) cells[i] = a.sg_cells[i];
   __syncthreads();
 }
 
@@ -902,7 +950,7 @@ struct PhotonPool {
 // Dynamic shared memory of a block: the warps' photon pools, then (recording pass) one
 // provenance slot per thread.
 template <int BLOCK, bool REC, bool STREAMS>
-constexpr size_t dyn_smem() {
+__host__ __device__ constexpr size_t dyn_smem() {
   return (BLOCK / 32) * sizeof(PhotonPool<STREAMS>) + (REC ? BLOCK * sizeof(Prov) : 0);
 }
 
@@ -912,7 +960,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
   extern __shared__ __align__(16) unsigned char dsm[];
   PhotonPool<STREAMS>* pools = reinterpret_cast<PhotonPool<STREAMS>*>(dsm);
   Prov* snaps = reinterpret_cast<Prov*>(dsm + (BLOCK / 32) * sizeof(PhotonPool<STREAMS>));
+  uint16_t* sgc = reinterpret_cast<uint16_t*>(dsm + dyn_smem<BLOCK, REC, STREAMS>());
+  __shared__ unsigned long long bsteps;  // the block's propagation steps
+  if (threadIdx.x == 0) bsteps = 0;
   load_tables(a, S);
+  load_cells(a, sgc);
   // launch sizes: from the parameters, or from device memory for replayed graphs
   const uint64_t num = a.dyn ? a.dyn[0] : a.num;
   const int nb = a.dyn ? (int)a.dyn[1] : a.nb;
@@ -934,8 +986,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
   int have = 0;             // warp-uniform: photons in the pool
   uint64_t sidx = gt;
   int hint = 0;
-  unsigned long long nsteps = 0;
-  unsigned int nan_steps = 0, capped = 0;
+  unsigned int nan_steps = 0;
   // REC: the gradient's recording pass (same step code as the replay, see AdjHook)
   typename std::conditional<REC, AdjHook, NoHook>::type hk;
   if constexpr (REC) {
@@ -1038,16 +1089,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       continue;
     }
     if (alive) {
-      step(a, S, ph, s, nan_steps, hk);
+      step(a, S, sgc, ph, s, nan_steps, hk);
       ph.steps++;
-      nsteps++;
-      if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) { ph.TOT = 0; capped++; }
-      if (ph.TOT == 0) alive = false;
+      if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) {  // the step cap (rare)
+        ph.TOT = 0;
+        atomicAdd(&a.ctrl->capped, 1u);
+      }
+      if (ph.TOT == 0) {  // the photon's steps go to the block's count
+        alive = false;
+        atomicAdd(&bsteps, (unsigned long long)ph.steps);
+      }
     }
   }
   if constexpr (!STREAMS) a.rs[gt] = (uint64_t)s.x | ((uint64_t)s.y << 32);
-  atomicAdd(&a.ctrl->steps, nsteps);
-  if (capped) atomicAdd(&a.ctrl->capped, capped);
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(&a.ctrl->steps, bsteps);
 }
 
 // Charge bin of a hit: its DOM, or with `events` > 0 (event, DOM) with the event taken
@@ -1069,8 +1125,11 @@ __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a
                                                  double* g_out, unsigned int* stats) {
   __shared__ SmemTables S;
   __shared__ double gbe[PPCB_MAXLYS], gba[PPCB_MAXLYS];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  uint16_t* sgc = reinterpret_cast<uint16_t*>(dsm);
   for (int i = threadIdx.x; i < PPCB_MAXLYS; i += blockDim.x) { gbe[i] = 0; gba[i] = 0; }
   load_tables(a, S);
+  load_cells(a, sgc);
   unsigned int nan_steps = 0, replayed = 0, unmatched = 0;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x) {
     const ppcb_hit h = hits[k];
@@ -1104,7 +1163,7 @@ __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a
     hk.prov_out = nullptr;
     hk.start = nullptr;
     while (!hk.done && ph.TOT != 0 && ph.steps < a.max_steps) {
-      step(a, S, ph, s, nan_steps, hk);
+      step(a, S, sgc, ph, s, nan_steps, hk);
       ph.steps++;
     }
     replayed++;
@@ -1131,7 +1190,20 @@ cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* pro
                            const float* wdom, const float2* wgrad, double* g_out, unsigned int* stats, int blocks,
                            cudaStream_t st) {
   if (nh == 0) return cudaSuccess;
-  k_adjoint<<<blocks, 256, 0, st>>>(a, hits, static_cast<const Prov*>(prov), nh, events, wdom, wgrad, g_out, stats);
+  // its static shared memory plus the string-proximity table exceed the default 48 KiB of
+  // dynamic shared memory: allow the largest table, once per device (before any capture)
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (!(done.load() & (1ull << (dev & 63)))) {
+    e = cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kSgMaxCells * sizeof(uint16_t)));
+    if (e != cudaSuccess) return e;
+    done.fetch_or(1ull << (dev & 63));
+  }
+  k_adjoint<<<blocks, 256, sg_cells_bytes(a), st>>>(a, hits, static_cast<const Prov*>(prov), nh, events, wdom, wgrad,
+                                                   g_out, stats);
   return cudaGetLastError();
 }
 
@@ -1196,9 +1268,13 @@ __global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos
 // static (deterministic = 1: thread streams, photon i on thread i mod T, nothing interleaves).
 // The dynamic shared-memory limit is a per-device function attribute: set it once on each
 // device (before any stream capture that launches the kernel there).
+// Dynamic shared memory: the photon pools (and provenance slots), then the
+// string-proximity cell entries; the attribute allows the largest table.
 template <int BLOCK, int MINB, bool REC, bool STREAMS>
 static cudaError_t launch_one(const KArgs& a, int blocks, cudaStream_t st) {
-  constexpr size_t dyn = dyn_smem<BLOCK, REC, STREAMS>();
+  constexpr size_t dmax = dyn_smem<BLOCK, REC, STREAMS>() + kSgMaxCells * sizeof(uint16_t);
+  const size_t dyn = dyn_smem<BLOCK, REC, STREAMS>() + sg_cells_bytes(a);
+  if (dyn > dmax) return cudaErrorInvalidValue;
   static std::atomic<uint64_t> done{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -1206,7 +1282,7 @@ static cudaError_t launch_one(const KArgs& a, int blocks, cudaStream_t st) {
   const uint64_t bit = 1ull << (dev & 63);
   if (!(done.load() & bit)) {
     e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, REC, STREAMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dyn);
+                             (int)dmax);
     if (e != cudaSuccess) return e;
     done.fetch_or(bit);
   }
@@ -1268,7 +1344,8 @@ cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size
 
 template <int BLOCK, int MINB>
 static int max_blocks(int* nb) {
-  constexpr size_t dyn = dyn_smem<BLOCK, false, true>();  // the larger pool (per-photon streams)
+  // the larger pool (per-photon streams) and the largest string-proximity table
+  constexpr size_t dyn = dyn_smem<BLOCK, false, true>() + kSgMaxCells * sizeof(uint16_t);
   cudaError_t e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, false, false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_propagate<BLOCK, MINB, false, false>, BLOCK, dyn);

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include "ppcb_types.h"
+#include "strgrid.h"
 
 namespace ppcb {
 
@@ -22,6 +23,10 @@ struct KArgs {
   const uint16_t* is;        // [CX*CY]       -> shared memory
   const int8_t* mcol;        // [CTX*CTY]     -> shared memory
   const float4* bfrt;        // [BFR_TAB+1]   -> shared memory
+  StrGridParams sg;          // string-proximity table (strgrid.h); sg.on = 0: no strings
+  const StrGroup* sg_groups; // [sg_ngroups]  -> shared memory
+  int sg_ngroups;
+  const uint16_t* sg_cells;  // [nx*ny]       -> shared memory (dynamic)
   // work
   const ppcb_bunch* bunches; // [nb]
   const uint64_t* bstart;    // [nb+1] first photon index of each bunch (exclusive prefix sum)

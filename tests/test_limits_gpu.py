@@ -44,11 +44,10 @@ def test_step_cap_stops_photons_and_is_reported(ice_small):
     c = _ctx(ice_small, max_steps=3)
     hits, info = c.propagate(_iso(num))
     assert info["photons"] == num
-    assert info["steps"] <= 3 * num
-    # nearly every photon lives longer than three steps, so nearly every one is capped
-    assert 0.9 * num < info["capped"] <= num, info
-    last, total = c.last_run()
-    assert total["capped"] >= info["capped"]
+    # most photons live longer than three steps: those are stopped after exactly three, the
+    # others ended (absorbed, or on a DOM) before the cap
+    assert num // 2 < info["capped"] <= num, info
+    assert 3 * info["capped"] <= info["steps"] <= 3 * num, info
 
     # the same through the device entry point: the count is in the caller's control block
     import torch
@@ -60,7 +59,7 @@ def test_step_cap_stops_photons_and_is_reported(ice_small):
     c.propagate_device(db.data_ptr(), ds.data_ptr(), 1, num, dh.data_ptr(), 1 << 16, ctrl.data_ptr())
     torch.cuda.synchronize()
     cc = T.Ctrl.from_buffer_copy(ctrl.cpu().numpy().tobytes())
-    assert 0.9 * num < cc.capped <= num and cc.steps <= 3 * num
+    assert num // 2 < cc.capped <= num and 3 * cc.capped <= cc.steps <= 3 * num
     c.close()
 
 
