@@ -488,7 +488,7 @@ def gradient_sample(local, events=64, photons=10_000_000, steps=3, plain_kernel=
     return out
 
 
-def run_fit(args, local):
+def fit_sample(local, iters=10, scale=1.0, plain_kernel=True):
     """Ice fit: 1024 flashers (log-uniform 1e5-1e7 photons, 12-fold LEDs at 30 degrees on
     distinct random DOMs) and 256 EM cascades (log-uniform 1e6-1e8 photons, vertex in
     |x|,|y|,|z| <= 500 m, isotropic directions); charges simulated with a hidden ice (be and
@@ -506,7 +506,7 @@ def run_fit(args, local):
     if not os.path.exists(os.path.join(ice, "cfg.txt")):
         synth.write("full", ice)
     rng = np.random.default_rng(55)
-    s = args.fit_scale
+    s = scale
 
     def ctx(seed):
         c = PPC()
@@ -558,7 +558,7 @@ def run_fit(args, local):
     lit_ba = np.abs(g0["g_ba"] * ba0) > 0.05 * np.abs(g0["g_ba"] * ba0).max()
     clk = Clocks(local)
     smooth = 3e-3 * float(obs.sum())  # penalty on layer-to-layer differences, scaled with the data
-    r = fit_ice(c, b, obs, events, iters=args.fit_iters, hit_cap=hit_cap, smooth=smooth)
+    r = fit_ice(c, b, obs, events, iters=iters, hit_cap=hit_cap, smooth=smooth)
     clocks = clk.stop()
     c.close()
 
@@ -583,7 +583,7 @@ def run_fit(args, local):
         "gpu_launches": 3 * r["evaluations"], "clocks": clocks, "accepted_steps": r["accepted"],
     }
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
-    if not args.no_plain_kernel and os.path.exists(exe):
+    if plain_kernel and os.path.exists(exe):
         path = os.path.join(tempfile.mkdtemp(), "fit_events.txt")
         with open(path, "w") as f:
             for i, k in enumerate(doms):
@@ -603,7 +603,11 @@ def run_fit(args, local):
                                                "reference CUDA kernel, one eout() per event (one forward timed, "
                                                "x 684)"}
             line["speedup_vs_fd_plain_kernel"] = fd_s / r["seconds_per_iteration"]
-    print(json.dumps(line))
+    return line
+
+
+def run_fit(args, local):
+    print(json.dumps(fit_sample(local, args.fit_iters, args.fit_scale, not args.no_plain_kernel)))
 
 
 def _plain_kernel_events(ev, local, timeout=1800):
@@ -634,7 +638,7 @@ def _plain_kernel_events(ev, local, timeout=1800):
             "photons": x["photons"], "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, one eout() per event"}
 
 
-def run_batched(args, local):
+def batched_sample(local, events=4096, steps=3, warmup=3, plain_kernel=True):
     """4096 events (log-uniform 1e3-1e7 photons; half flashers on random DOMs, 12-fold at
     30 degrees, half cascades) in one graph-replayed launch, against the reference's CUDA
     kernel propagating the same events one eout() at a time.  `by_decade` repeats the
@@ -654,33 +658,33 @@ def run_batched(args, local):
     c.choose(local)
     c.ini()
     oms = c.tables()["oms"]
-    ev = W.batched_events(oms, n_events=args.events, seed=11)
+    ev = W.batched_events(oms, n_events=events, seed=11)
     photons = int(ev["num"].sum())
     # the per-decade comparisons below reuse the batch: size it for the largest of the runs
     dec_ev = {lo: W.batched_events(oms, n_events=512, lo=lo, hi=10 * lo, seed=int(lo)) for lo in (1e3, 1e4, 1e5, 1e6)}
     most = max([photons] + [int(e["num"].sum()) for e in dec_ev.values()])
-    nmax = max(args.events, 512)
+    nmax = max(events, 512)
     b = Batch(c, max_events=nmax, max_bunches=nmax, hit_capacity=int(most * 0.02) + 66 * nmax)
-    tune = b.autotune(ev, args.events, sample_photons=50_000_000)
-    for _ in range(max(1, args.warmup - 2)):
-        b.run(ev, args.events, hits_per_photon=0.02)
+    tune = b.autotune(ev, events, sample_photons=50_000_000)
+    for _ in range(max(1, warmup - 2)):
+        b.run(ev, events, hits_per_photon=0.02)
     runs = []
     clk = Clocks(local)
-    for _ in range(args.steps):
-        runs.append(b.run(ev, args.events, hits_per_photon=0.02))
+    for _ in range(steps):
+        runs.append(b.run(ev, events, hits_per_photon=0.02))
     clocks = clk.stop()
     graph_s = sum(r["graph_ms"] for r in runs) / 1000.0
     line = {
-        "metric": "events/s", "value": args.events * len(runs) / graph_s, "unit": "events/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * graph_s / len(runs),
+        "metric": "events/s", "value": events * len(runs) / graph_s, "unit": "events/s", "n_gpus": 1,
+        "steps": steps, "warmup": warmup, "ms_per_step": 1000.0 * graph_s / len(runs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.events} events, log-uniform 1e3-1e7 photons, 50% flashers (12-fold, 30 deg) "
+        "config": {"workload": f"{events} events, log-uniform 1e3-1e7 photons, 50% flashers (12-fold, 30 deg) "
                                f"50% EM cascades, full detector", "photons_per_step": photons,
                    "launch": f"graph replay, autotuned {tune['threads']}x{tune['blocks_per_sm']} "
                              f"refill {tune['refill_below']}"},
         "photons_per_s": photons * len(runs) / graph_s,
         "overflowed_events": max(r["overflowed"] for r in runs),
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 3 * steps,
         "clocks": clocks,
     }
     decades = []
@@ -693,7 +697,7 @@ def run_batched(args, local):
     b.close()
     c.close()
     torch.cuda.empty_cache()
-    if not args.no_plain_kernel:
+    if plain_kernel:
         pk = _plain_kernel_events(ev, local)
         if pk:
             line["plain_kernel"] = pk
@@ -706,7 +710,11 @@ def run_batched(args, local):
     for d in decades:
         del d["_ev"]
     line["by_decade"] = decades
-    print(json.dumps(line))
+    return line
+
+
+def run_batched(args, local):
+    print(json.dumps(batched_sample(local, args.events, args.steps, args.warmup, not args.no_plain_kernel)))
 
 
 def run_reference(args, rank, world):
@@ -835,29 +843,44 @@ def run_ours(args, rank, world, local):
     e2e_value = world * photons * args.steps / e2e_total
     launch_ms = total_ms / args.steps
     steps_per_launch = steps_done / args.steps
-    # roofline: FP32/SFU issue.  Per photon-step, the FP32 operations (thread-level FADD +
-    # FMUL + 2 x FFMA) and the special-function-unit thread instructions, both counted by ncu
-    # on this kernel and this workload's first cascade (profiles/k_propagate_roofline.md),
-    # x photon-steps of the launch / its event-timed duration; against the FFMA and SFU
-    # throughputs measured on this GPU by the library's own loops (ppcb_fp32_peak,
-    # ppcb_sfu_peak).  The roofline fraction is the larger of the two.
+    # roofline: the FP32/SFU issue roofline.  Algorithmic operations per photon-step (the
+    # oracle's event counts on this workload times a per-event operation table counted from
+    # the reference's source: oracle/algorithmic_ops.py -> profiles/k_propagate_algorithmic.json)
+    # x this launch's photon-steps / its event-timed duration, against the FFMA and SFU
+    # throughputs measured on this GPU by the library's own loops (the driver-measured peaks
+    # have no FP32 or SFU figure).  Beside it, the same with the kernel's executed FP32 and
+    # SFU instructions per step from its ncu capture (profiles/k_propagate_cascade.json).
     from ppc_b200.api import fp32_peak, sfu_peak
-    ops_per_step = args.fp32_ops_per_step
-    achieved = ops_per_step * steps_per_launch / (launch_ms / 1000.0) / 1e12
+    alg = _profile_json("k_propagate_algorithmic.json")
+    exe = _profile_json("k_propagate_cascade.json")
     props = torch.cuda.get_device_properties(local)
-    peak = fp32_peak(local, repeats=5)
-    sfu_achieved = args.sfu_ops_per_step * steps_per_launch / (launch_ms / 1000.0) / 1e12
-    sfu_pk = sfu_peak(local, repeats=5)
-    fp32 = {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "ops_per_photon_step": ops_per_step,
-            "peak_source": f"measured: FFMA loop on all {props.multi_processor_count} SMs (ppcb_fp32_peak); "
-                           "no FP32 figure is among the driver-measured peaks"}
-    sfu = {"achieved": sfu_achieved, "peak": sfu_pk, "unit": "Tops/s", "frac": sfu_achieved / sfu_pk,
-           "ops_per_photon_step": args.sfu_ops_per_step,
-           "peak_source": f"measured: reciprocal-square-root loop on all {props.multi_processor_count} SMs "
-                          "(ppcb_sfu_peak)"}
-    top = sfu if sfu["frac"] > fp32["frac"] else fp32
-    traffic = args.dram_bytes_per_step * steps_per_launch
+    pk_fp32, pk_sfu = fp32_peak(local, repeats=5), sfu_peak(local, repeats=5)
+    sps = steps_per_launch / (launch_ms / 1000.0)
+
+    def fracs(fp32_ops, sfu_ops):
+        f = {"fp32": {"ops_per_photon_step": fp32_ops, "achieved": fp32_ops * sps / 1e12, "peak": pk_fp32,
+                      "unit": "TFLOP/s"},
+             "sfu": {"ops_per_photon_step": sfu_ops, "achieved": sfu_ops * sps / 1e12, "peak": pk_sfu, "unit": "Tops/s"}}
+        for v in f.values():
+            v["frac"] = v["achieved"] / v["peak"]
+        return f
+
+    algo = fracs(alg["fp32_ops_per_step"], alg["sfu_ops_per_step"]) if alg else None
+    execd = fracs(exe["fp32_ops_per_step"], exe["sfu_ops_per_step"]) if exe else None
+    base = algo or execd
+    top = base["sfu"] if base["sfu"]["frac"] >= base["fp32"]["frac"] else base["fp32"]
+    traffic = exe["dram_bytes_per_step"] * steps_per_launch if exe else None
+    roofline = {"bound": "sfu" if top is base["sfu"] else "fp32", "achieved": top["achieved"], "peak": top["peak"],
+                "unit": top["unit"], "frac": top["frac"], "traffic": traffic,
+                "kind": "FP32/SFU issue roofline on algorithmic ops (oracle event counts x per-event table of "
+                        "gpu/pro.cu), the larger fraction",
+                "peak_source": f"measured on this GPU: FFMA and reciprocal-square-root loops on all "
+                               f"{props.multi_processor_count} SMs (ppcb_fp32_peak, ppcb_sfu_peak)",
+                "algorithmic": algo, "executed": execd,
+                "traffic_source": (f"ncu dram bytes per photon-step ({exe['dram_bytes_per_step']:.3g} B) scaled by "
+                                   "this launch's photon-steps") if exe else None}
+    if exe:
+        roofline["issue_ncu"] = exe.get("issue")
     h2d = 64 + 16
     d2h = 32 * (e2e_hits / max(1, args.steps)) + 56
     line = {
@@ -873,28 +896,18 @@ def run_ours(args, rank, world, local):
         "gpu_launches": args.steps,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h), "gpu_launches": args.steps},
-        "roofline": {"bound": "sfu" if top is sfu else "fp32", "achieved": top["achieved"], "peak": top["peak"],
-                     "unit": top["unit"], "frac": top["frac"], "traffic": traffic,
-                     "peak_source": top["peak_source"],
-                     "kind": "FP32/SFU issue roofline: the larger of the FP32 and SFU fractions",
-                     "fp32": fp32, "sfu": sfu,
-                     "traffic_source": f"ncu dram__bytes_read+write per photon-step ({args.dram_bytes_per_step:.1f} B) "
-                                       "on a 1e7-photon launch, scaled by this launch's photon-steps",
-                     "hbm": {"achieved_gbs": traffic / (launch_ms / 1000.0) / 1e9,
-                             "peak_gbs": _peaks().get("hbm_gbs"), "peak_source": "of measured (MEASURED_PEAKS.json)"},
-                     # the binding limit, from the ncu capture of this kernel (not measured live):
-                     # issue slots busy and the FP32 (FMA), ALU and SFU (XU) pipes' share of peak
-                     "issue_ncu": {"issue_active": 0.846, "fma_pipe": 0.356, "alu_pipe": 0.437, "xu_pipe": 0.352,
-                                   "threads_per_warp_inst": 22.2,
-                                   "source": "profiles/k_propagate_cascade.md (ncu --set full, 1e7-photon cascade)"}},
+        "roofline": roofline,
         "clocks": clocks,
     }
+    summary = {"photons_per_s": value, "photon_steps_per_s": line["photon_steps_per_s"], "e2e_photons_per_s": e2e_value,
+               "roofline_frac": top["frac"]}
     # the comparisons below are single-GPU figures: a multi-GPU run reports throughput only
     single = world == 1
-    if single and not args.no_plain_kernel:
+    if single:
         del d_hits, flush
         torch.cuda.empty_cache()
         c.close()
+    if single and not args.no_plain_kernel:
         pk = plain_kernel_sample(timed_cascades, photons, local)
         if pk:
             line["plain_kernel"] = {"value": pk["value"], "unit": "photons/s", "device_ms": pk["device_ms"],
@@ -902,12 +915,30 @@ def run_ours(args, rank, world, local):
                                     "kind": "reference CUDA kernel gpu/pro.cu, sm_100a, gpu/Makefile flags, "
                                             "the timed steps' cascades, one eout() each",
                                     "speedup": value / pk["value"]}
+            summary["plain_kernel_speedup"] = value / pk["value"]
     if single and not args.no_gradient:
-        if args.no_plain_kernel:
-            del d_hits, flush
-            torch.cuda.empty_cache()
-            c.close()
-        line["gradient"] = gradient_sample(local, plain_kernel=not args.no_plain_kernel)
+        g = gradient_sample(local, plain_kernel=not args.no_plain_kernel)
+        line["gradient"] = g
+        summary["gradient_evals_per_s"] = g["evals_per_s"]
+        summary["gradient_backward_over_forward"] = g["backward_over_forward"]
+    if single and not args.no_batched:
+        bt = batched_sample(local, events=4096, steps=2, warmup=3, plain_kernel=not args.no_plain_kernel)
+        for k in ("metric", "unit", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype", "data"):
+            bt.pop(k, None)
+        line["batched"] = bt
+        summary["batched_events_per_s"] = bt["value"]
+        if "speedup_vs_plain_kernel" in bt:
+            summary["batched_plain_kernel_events_per_s"] = bt["plain_kernel"]["events_per_s"]
+            summary["batched_speedup_vs_plain_kernel"] = bt["speedup_vs_plain_kernel"]
+    if single and not args.no_fit:
+        ft = fit_sample(local, iters=args.fit_iters, scale=args.fit_scale, plain_kernel=not args.no_plain_kernel)
+        for k in ("n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype", "data"):
+            ft.pop(k, None)
+        line["fit"] = ft
+        summary["fit_seconds_per_iteration"] = ft["value"]
+        summary["fit_photon_scale"] = args.fit_scale
+        if "speedup_vs_fd_plain_kernel" in ft:
+            summary["fit_speedup_vs_fd_plain_kernel"] = ft["speedup_vs_fd_plain_kernel"]
     if single and not args.no_stages:
         line["stages"] = stages_sample(local)
     if single and not args.no_cpu_baseline:
@@ -930,6 +961,7 @@ def run_ours(args, rank, world, local):
         if cands:
             best = max(cands, key=lambda x: x["value"])
             line["cpu_baseline"] = best
+            summary["cpu_baseline_photons_per_s"] = best["value"]
             if gpu_build and gpu_build is not best:
                 others["gpu_cpu_build_all_cores"] = gpu_build
             if par and par is not best:
@@ -941,7 +973,17 @@ def run_ours(args, rank, world, local):
                                                           "CPU build (oracle/_ref/ref_harness_fm)"}
         if others:
             line["cpu_baselines_other"] = others
+    line["summary"] = summary  # last: the headline figures at the end of the line
     print(json.dumps(line))
+
+
+def _profile_json(name):
+    """A committed measurement summary under profiles/ (None when absent)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            return json.load(f)
+    except Exception:
+        return None
 
 
 def main():
@@ -952,20 +994,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--photons", type=int, default=PHOTONS)
     ap.add_argument("--ref-photons", type=int, default=200_000)
-    ap.add_argument("--fp32-ops-per-step", type=float, default=402.8)
-    ap.add_argument("--sfu-ops-per-step", type=float, default=50.6)
-    ap.add_argument("--dram-bytes-per-step", type=float, default=0.007)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-plain-kernel", action="store_true", help="skip the reference CUDA kernel comparison")
     ap.add_argument("--no-gradient", action="store_true", help="skip the ice-gradient evaluation")
     ap.add_argument("--no-stages", action="store_true", help="skip the back end, likelihood and front end stages")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-events comparison (4096 events)")
+    ap.add_argument("--no-fit", action="store_true", help="skip the ice-fit iterations")
     ap.add_argument("--cascade", type=lambda t: [float(x) for x in t.split(",")], default=None,
                     help="x,y,z,nx,ny,nz: one fixed cascade for every step instead of random ones (profiling)")
     ap.add_argument("--config", default="cascade", choices=["cascade", "batched", "fit"],
                     help="cascade: the headline workload; batched: 4096 events in one launch; "
                          "fit: L-BFGS ice fit over 1280 events")
-    ap.add_argument("--fit-iters", type=int, default=10)
+    ap.add_argument("--fit-iters", type=int, default=3)
     ap.add_argument("--fit-scale", type=float, default=1.0, help="photon counts of the fit workload x this")
     ap.add_argument("--events", type=int, default=4096)
     args = ap.parse_args()

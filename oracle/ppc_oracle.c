@@ -19,6 +19,12 @@
 #define OMR PPCB_OMR
 static const float fcv = FPI / 180.f;
 
+/* Event counters of ppco_propagate (the algorithmic work of the propagation: steps, layer
+ * crossings, string and DOM tests, hits, birefringence and scattering evaluations). */
+static ppco_counts g_cnt;
+void ppco_counts_reset(void) { memset(&g_cnt, 0, sizeof(g_cnt)); }
+void ppco_counts_get(ppco_counts* out) { *out = g_cnt; }
+
 /* std::min / std::max argument-order semantics */
 static inline float mnf(float a, float b) { return b < a ? b : a; }
 static inline float mxf(float a, float b) { return a < b ? b : a; }
@@ -354,14 +360,16 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
   const uint32_t niw = f->i;
   int om = f->fla;
   const int ofla = f->ofla;
+  g_cnt.photons++;
   int old = -1;
   float TOT = -logf(ppco_xrnd(s)), SCA = 0;
   if (ofla < -1) TOT = 0;
   uint64_t steps = 0;
   for (;;) {
     steps++;
+    g_cnt.steps++;
     float sqd = 0;
-    if (SCA == 0) { SCA = -logf(ppco_xrnd(s)); old = om; }
+    if (SCA == 0) { SCA = -logf(ppco_xrnd(s)); old = om; g_cnt.sca_draws++; }
     float sca, tot;
     int sign = n.z < 0 ? -1 : 1;
     float anz = sign * n.z;
@@ -405,6 +413,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
           ais -= wsca(t, wl, J) * del; aia -= wabs(t, wl, J) * del;
           ahx = edh;
           J += sign;
+          g_cnt.crossings++;
         } else {
           sca += dsca; tot += dtot;
           break;
@@ -427,6 +436,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
           unsigned short m = t->ls[k];
           const ppcb_line* sl = &t->sc[m & 0x7fff];
           k = (m & 0x8000) ? 0x8000 : k + 1;
+          g_cnt.strings_tested++;
           float b = 0, c = 0, dr;
           dr = sl->x - r.x; b += n.x * dr; c += dr * dr;
           dr = sl->y - r.y; b += n.y * dr; c += dr * dr;
@@ -447,7 +457,9 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
               else { zl = h2; zh = h1; }
               int n1, n2;
               dom_window(sl, zl, zh, &n1, &n2);
+              g_cnt.strings_passed++;
               for (int l = n1; l <= n2; l++) if (l != old) {
+                g_cnt.doms_tested++;
                 const ppcb_dom* dom = &t->oms[l];
                 float a = 0, bb = 0, cc = 0, dd;
                 float fq = dom->F > 0 ? sq(1 / dom->F) : 0;
@@ -492,6 +504,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
     float fin = mnf(del, hi);
     int hole = fin < sca;
     if (hole) {  /* truncated step: overburden by layers, hole-ice column, gpu/pro.cu:677-717 */
+      g_cnt.truncated++;
       {
         float xs = 0, xa = 0;
         float y = z + n.z * fin / edh;
@@ -539,6 +552,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
         h.dth = acosf(mnf(mxf(dz / (e->xR * dom->R * dom->F), -1.f), 1.f));
         h.dph = atan2f(dy, dx);
         uint64_t jh = (*nhit)++;
+        g_cnt.hits++;
         if (jh < cap) hits[jh] = h;
         if (e->xR == 1) TOT = 0;
         else old = om;
@@ -548,6 +562,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
     if (TOT < XXX) TOT = 0;
     else {
       if (e->sum > 0 && fin > 0) {  /* birefringence diffusion, gpu/pro.cu:757-836 */
+        g_cnt.bfr++;
         float ra, rb;
         if (I == J) { ra = fin * t->az[I].ra; rb = fin * t->az[I].rb; }
         else {
@@ -556,7 +571,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
           float g = 0.5f + sign * (y - J);
           ra = h * t->az[I].ra + g * t->az[J].ra;
           rb = h * t->az[I].rb + g * t->az[J].rb;
-          for (int i = I + sign; i != J; i += sign) { ra += t->az[i].ra; rb += t->az[i].rb; }
+          for (int i = I + sign; i != J; i += sign) { ra += t->az[i].ra; rb += t->az[i].rb; g_cnt.bfr_layers++; }
           float ff = edh / anz;
           ra *= ff; rb *= ff;
         }
@@ -582,6 +597,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
         float dnx = sx * g1 + mx;
         float dny = sy * g2;
         if (del <= hi) {  /* curved path within the segment */
+          g_cnt.bfr_curved++;
           grnd2(&g1, &g2, s);
           /* the CPU build's rsqrtf is the textual macro 1/sqrtf (gpu/pro.cu:6), so this
              product becomes a division there: keep that rounding */
@@ -620,6 +636,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
         else { sf = e->sf; g = e->g; gr = e->gr; }
         float xi = ppco_xrnd(s);
         if (xi > sf) {
+          g_cnt.scatter_hg++;
           xi = (1 - xi) / (1 - sf);
           xi = 2 * xi - 1;
           if (g != 0) {
@@ -627,6 +644,7 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
             xi = (ga * ga - sq(1 - g)) / (2 * g);
           }
         } else {
+          g_cnt.scatter_sam++;
           xi /= sf;
           xi = 2 * (1 - powf(xi, gr));
         }

@@ -34,6 +34,15 @@ typedef struct ppco_tables {
 /* MWC stream: x,y state words, a multiplier (gpu/pro.cu:47-57) */
 typedef struct ppco_rng { uint32_t x, y, a; } ppco_rng;
 
+/* Events counted by ppco_propagate since the last ppco_counts_reset. */
+typedef struct ppco_counts {
+  uint64_t photons, steps, sca_draws, crossings;
+  uint64_t strings_tested, strings_passed, doms_tested, hits, truncated;
+  uint64_t bfr, bfr_curved, bfr_layers, scatter_hg, scatter_sam;
+} ppco_counts;
+void ppco_counts_reset(void);
+void ppco_counts_get(ppco_counts* out);
+
 /* phase-1 photon record (gpu/ini.cxx:391-397) */
 typedef struct ppco_pbuf {
   float r[4], n[4];

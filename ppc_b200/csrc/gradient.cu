@@ -111,8 +111,14 @@ Engine::Grad Engine::gradient(const ppcb_bunch* b, int nb, uint32_t events, cons
   // the recording kernel's shape: the engine's block size (864 threads, one block per SM, or
   // 256 threads, three per SM), all blocks resident at once (a static photon order must not
   // leave a second wave of blocks), and no more threads than streams
-  const int tpb = threads_per_block == 864 ? 864 : 256;
-  const int per_sm = tpb == 864 ? 1 : propagate_max_blocks_per_sm(256);
+  // (the 864-thread shape falls back to 256 threads when it cannot be resident)
+  int tpb = threads_per_block == 864 ? 864 : 256;
+  int per_sm = propagate_rec_blocks_per_sm(tpb, a.deterministic);
+  if (tpb == 864 && (per_sm < 1 || g.T / 864 < 1)) {
+    tpb = 256;
+    per_sm = propagate_rec_blocks_per_sm(tpb, a.deterministic);
+  }
+  if (per_sm < 1 || g.T / tpb < 1) throw Error("gradient: the recording kernel does not fit on this device", 2);
   const int rec_blocks = std::min(g.prop.multiProcessorCount * per_sm, g.T / tpb);
   check(launch_propagate(a, LaunchShape{rec_blocks, tpb}, st), "recording launch");
   check(cudaEventRecord(e1, st), "event");

@@ -1352,6 +1352,29 @@ static int max_blocks(int* nb) {
   return e == cudaSuccess ? *nb : 0;
 }
 
+// Resident blocks per SM of the gradient's recording kernel (its provenance slots and the
+// largest string-proximity table included); 0 when the shape does not fit.
+template <int BLOCK, int MINB, bool STREAMS>
+static int rec_blocks(int* nb) {
+  constexpr size_t dyn = dyn_smem<BLOCK, true, STREAMS>() + kSgMaxCells * sizeof(uint16_t);
+  cudaError_t e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, true, STREAMS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_propagate<BLOCK, MINB, true, STREAMS>, BLOCK, dyn);
+  if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+  return *nb;
+}
+
+int propagate_rec_blocks_per_sm(int threads, int deterministic) {
+  int nb = 0;
+  const bool streams = deterministic != 1;
+  switch (threads) {
+    case 256: return streams ? rec_blocks<256, 3, true>(&nb) : rec_blocks<256, 3, false>(&nb);
+    case 864: return streams ? rec_blocks<864, 1, true>(&nb) : rec_blocks<864, 1, false>(&nb);
+    default: return 0;
+  }
+}
+
 int propagate_max_blocks_per_sm(int threads) {
   int nb = 0;
   switch (threads) {

@@ -75,5 +75,6 @@ cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* cou
 constexpr size_t kProvBytes = 64;  // provenance record per hit slot of the gradient's recording pass
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local);
 int propagate_max_blocks_per_sm(int threads);
+int propagate_rec_blocks_per_sm(int threads, int deterministic);
 
 }  // namespace ppcb
