@@ -405,6 +405,16 @@ def f2k_sources(text, first_segment=1):
     return out[:n.value], lines.value
 
 
+def good_list_bad(data, good):
+    """The DOMs that a good-DOM list turns bad: those with observed pulses that are not on
+    the list (llh/llh.cxx:774-781 inserts each such DOM into the bad set when it reads its
+    pulses), as (str, om) rows."""
+    g = {(int(s), int(o)) for s, o in np.asarray(good, np.int32).reshape(-1, 2)}
+    d = np.ascontiguousarray(data, T.LLH_HIT_DTYPE)
+    keys = sorted({(int(s), int(o)) for s, o in zip(d["str"], d["om"])} - g)
+    return np.array(keys, np.int32).reshape(-1, 2)
+
+
 class Likelihood:
     """DirectFit's likelihood (llh/llh.cxx:419-662, 1075-1082) with the simulation side on
     the GPU (ppcb_llh_*).  `data`: observed pulses (LLH_HIT_DTYPE: str, om, t, q), prepared
@@ -413,9 +423,11 @@ class Likelihood:
     acceptance (as PPC.accept with the same seed) and returns fllh(dt, nsim) for every
     shift dt.  Options (DirectFit's names and defaults): lbin (0: automatic), sig (0.10),
     qmin (0.1), qsat (500), drep (1), peak, mono, norm, unh (0), flasher, fla_str,
-    fla_om (0), fsep (1)."""
+    fla_om (0), fsep (1).  `good`: the good-DOM list (DirectFit's `set` file,
+    llh/llh.cxx:741-744): when given, pulses on other DOMs are dropped and those DOMs are
+    treated as bad, as the reference does while reading the pulses (llh/llh.cxx:774-781)."""
 
-    def __init__(self, ctx, data, windows=None, bad=None, device=0, **opts):
+    def __init__(self, ctx, data, windows=None, bad=None, device=0, good=None, **opts):
         from ._lib import LlhOpts
         o = LlhOpts()
         check(lib().ppcb_llh_default_opts(C.byref(o)))
@@ -427,6 +439,8 @@ class Likelihood:
         win = np.ascontiguousarray(windows if windows is not None else np.zeros(0, T.LLH_WINDOW_DTYPE),
                                    T.LLH_WINDOW_DTYPE)
         badk = np.ascontiguousarray(bad if bad is not None else np.zeros((0, 2)), np.int32).reshape(-1, 2)
+        if good is not None and len(good):
+            badk = np.concatenate([badk, good_list_bad(data, good)])
         self._ctx = ctx  # keeps the context alive
         self._h = C.c_void_p()
         check(lib().ppcb_llh_create(ctx._c, int(device), _p(data), len(data), _p(win) if len(win) else None,
