@@ -47,6 +47,7 @@ struct SmemTables {
   int8_t mcol[PPCB_CTX * PPCB_CTY];
   float4 bfrt[PPCB_BFR_TAB + 1];  // birefringence angular functions (sx, sy, mx, -)
   StrGroup sgg[PPCB_NSTR];        // string-proximity table: string axes (strgrid.h)
+  float4 azr[PPCB_MAXLYS];        // per layer 1/k1, 1/k2, 1/(k1 k2): the scattering's frame divisions
 };
 
 // ---------------------------------------------------------------- IEEE helpers
@@ -885,13 +886,13 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
         float n2 = (-e.azy * n.x + e.azx * n.y) * k2;
         n.x = n1 * e.azx - n2 * e.azy;
         n.y = n1 * e.azy + n2 * e.azx;
-        n.z /= okz;
+        n.z *= S.azr[J].z;
         normalize3(n);
       }
       rotate(xi, sqrtf(xi * (2 - xi)), n, s);
       if (!hole) {
-        float n1 = (e.azx * n.x + e.azy * n.y) / k1;
-        float n2 = (-e.azy * n.x + e.azx * n.y) / k2;
+        float n1 = (e.azx * n.x + e.azy * n.y) * S.azr[J].x;
+        float n2 = (-e.azy * n.x + e.azx * n.y) * S.azr[J].y;
         n.x = n1 * e.azx - n2 * e.azy;
         n.y = n1 * e.azy + n2 * e.azx;
         n.z *= okz;
@@ -912,6 +913,10 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
   for (int i = t; i < PPCB_CTX * PPCB_CTY; i += nt) S.mcol[i] = a.mcol[i];
   for (int i = t; i <= PPCB_BFR_TAB; i += nt) S.bfrt[i] = a.bfrt[i];
   for (int i = t; i < a.sg_ngroups; i += nt) S.sgg[i] = a.sg_groups[i];
+  for (int i = t; i < a.p.size; i += nt) {
+    const ppcb_aniz z = a.az[i];
+    S.azr[i] = make_float4(__fdividef(1.f, z.k1), __fdividef(1.f, z.k2), __fdividef(1.f, z.k1 * z.k2), 0.f);
+  }
   __syncthreads();
 }
 
@@ -984,8 +989,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
   bool alive = false;
   bool exhausted = false;   // warp-uniform: no photons left to sample
   int have = 0;             // warp-uniform: photons in the pool
-  uint64_t sidx = gt;
-  int hint = 0;
+  // rarely used per-thread state in shared memory instead of registers: the next photon
+  // index in the static order and the last bunch found
+  __shared__ uint64_t s_sidx[BLOCK];
+  __shared__ int s_hint[BLOCK];
+  s_sidx[threadIdx.x] = gt;
+  s_hint[threadIdx.x] = 0;
   unsigned int nan_steps = 0;
   // REC: the gradient's recording pass (same step code as the replay, see AdjHook)
   typename std::conditional<REC, AdjHook, NoHook>::type hk;
@@ -1006,9 +1015,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       unsigned long long base = 0;
       int ngen = 0;
       if (a.deterministic == 1) {  // photon i on thread i mod T, as the oracle sequences it
-        gen = !alive && sidx < num;
-        gidx = sidx;
-        if (!alive) sidx += T;
+        gen = !alive && s_sidx[threadIdx.x] < num;
+        gidx = s_sidx[threadIdx.x];
+        if (!alive) s_sidx[threadIdx.x] += T;
       } else if ((have < __popc(dead) || have < a.refill_below) && !exhausted) {
         ngen = 32 - have;
         if (lane == 0) base = atomicAdd(&a.ctrl->next, (unsigned long long)ngen);
@@ -1020,7 +1029,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       Photon g;
       uint4 gst = make_uint4(0, 0, 0, 0);
       if (gen) {
-        hint = find_bunch(a, nb, gidx, hint);
+        const int hint = find_bunch(a, nb, gidx, s_hint[threadIdx.x]);
+        s_hint[threadIdx.x] = hint;
         if constexpr (STREAMS) {  // the photon's own stream; the lane's s is left alone
           Rng sg;
           const uint32_t m = (uint32_t)(gidx % nmul);
@@ -1041,7 +1051,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
           alive = true;
           if constexpr (STREAMS) { s.x = gst.x; s.y = gst.y; mi = gst.z; s.a = a.rm[mi]; }
         }
-        exhausted = __all_sync(FULL, sidx >= num);
+        exhausted = __all_sync(FULL, s_sidx[threadIdx.x] >= num);
       } else {
         if (gen) {
           const int slot = have + lane;
