@@ -560,6 +560,15 @@ def fit_sample(local, iters=10, scale=1.0, plain_kernel=True):
     smooth = 3e-3 * float(obs.sum())  # penalty on layer-to-layer differences, scaled with the data
     r = fit_ice(c, b, obs, events, iters=iters, hit_cap=hit_cap, smooth=smooth)
     clocks = clk.stop()
+    # one evaluation at the fitted ice through the graph and through the eager path
+    G = c.gradient_graph(b, obs, events=events, hit_cap=hit_cap)
+    t0 = time.perf_counter()
+    G.run(r["be"].astype(np.float32), r["ba"].astype(np.float32), counts=False)
+    eval_graph = time.perf_counter() - t0
+    G.close()
+    t0 = time.perf_counter()
+    c.gradient(b, observed=obs, events=events, hit_cap=hit_cap)
+    eval_eager = time.perf_counter() - t0
     c.close()
 
     def rms(x, t, m):
@@ -580,7 +589,10 @@ def fit_sample(local, iters=10, scale=1.0, plain_kernel=True):
         "recovery": {"lit_layers_be": int(lit_be.sum()), "lit_layers_ba": int(lit_ba.sum()),
                      "rms_rel_error_be": [rms(be0, be_t, lit_be), rms(r["be"], be_t, lit_be)],
                      "rms_rel_error_ba": [rms(ba0, ba_t, lit_ba), rms(r["ba"], ba_t, lit_ba)]},
-        "gpu_launches": 3 * r["evaluations"], "clocks": clocks, "accepted_steps": r["accepted"],
+        "gpu_launches": 5 * r["evaluations"], "clocks": clocks, "accepted_steps": r["accepted"],
+        "evaluation_s": {"graph": eval_graph, "eager": eval_eager,
+                         "kind": "one likelihood-and-gradient evaluation at the fitted ice: the CUDA graph "
+                                 "(forward, histogram, weights, replay) against the eager calls"},
     }
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_harness")
     if plain_kernel and os.path.exists(exe):

@@ -223,6 +223,18 @@ int ppcb_get_ice(ppcb_ctx* c, float* be, float* ba, int32_t* size);
 int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t events, const float* observed,
                   const float* weights, double scale, uint64_t hit_cap, uint32_t* counts, double* g_be, double* g_ba,
                   ppcb_grad_info* info);
+/* One ice-fit iteration as a CUDA graph: the bunches and observed charges are fixed at
+ * creation; each ppcb_gradgraph_run sets new be/ba (NULL keeps), uploads the rebuilt table
+ * and replays the recording pass, histogram, Poisson weights and log-likelihood, and the
+ * replay of the detected photons, with the hit count kept on the device between them.
+ * Same results as ppcb_gradient with `observed` (the log-likelihood summed in another
+ * order).  Destroy it before its context. */
+typedef struct ppcb_gradgraph ppcb_gradgraph;
+int ppcb_gradgraph_create(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t events, const float* observed,
+                          double scale, uint64_t hit_cap, ppcb_gradgraph** out);
+int ppcb_gradgraph_run(ppcb_gradgraph* g, const float* be, const float* ba, uint32_t* counts, double* g_be,
+                       double* g_ba, ppcb_grad_info* info);
+int ppcb_gradgraph_destroy(ppcb_gradgraph* g);
 
 /* ---- propagation that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device memory while

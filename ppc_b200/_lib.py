@@ -81,7 +81,7 @@ EXPORTS = [
     "ppcb_fp32_peak", "ppcb_accept_device", "ppcb_accept", "ppcb_llh_default_opts", "ppcb_llh_create",
     "ppcb_llh_destroy", "ppcb_llh_get_info", "ppcb_llh_blocks", "ppcb_llh_eval_device", "ppcb_llh_eval",
     "ppcb_sources_device", "ppcb_sources", "ppcb_f2k_sources", "ppcb_back_end", "ppcb_sfu_peak",
-    "ppcb_string_grid_probe",
+    "ppcb_string_grid_probe", "ppcb_gradgraph_create", "ppcb_gradgraph_run", "ppcb_gradgraph_destroy",
 ]
 
 
@@ -133,6 +133,9 @@ def lib():
         "ppcb_generate_device": (i32, [vp, i32, vp, vp, i32, u64, vp, vp]),
         "ppcb_index_probe_device": (i32, [vp, i32, vp, i32, vp, vp, vp]),
         "ppcb_string_grid_probe": (i32, [vp, vp, i32, vp]),
+        "ppcb_gradgraph_create": (i32, [vp, vp, i32, u32, vp, f64, u64, vp]),
+        "ppcb_gradgraph_run": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+        "ppcb_gradgraph_destroy": (i32, [vp]),
         "ppcb_propagate_noalloc": (i32, [vp, i32, vp, i32, u64, vp, u64, vp, vp]),
         "ppcb_batch_create": (i32, [vp, i32, u32, u32, u64, P(vp)]),
         "ppcb_batch_destroy": (i32, [vp]),

@@ -319,9 +319,15 @@ def _ice_methods():
         return {"ll": gi.ll, "counts": counts, "g_be": g_be, "g_ba": g_ba,
                 "info": {k: getattr(gi, k) for k, _ in GradInfo._fields_}}
 
+    def gradient_graph(self, bunches, observed, events=0, scale=1.0, hit_cap=None):
+        """One fit iteration as a CUDA graph over fixed bunches and observed charges
+        (ppcb_gradgraph_*): GradGraph.run(be, ba) returns what gradient(observed=...) does."""
+        return GradGraph(self, bunches, observed, events, scale, hit_cap)
+
     PPC.set_ice = set_ice
     PPC.get_ice = get_ice
     PPC.gradient = gradient
+    PPC.gradient_graph = gradient_graph
 
 
 _ice_methods()
@@ -403,6 +409,53 @@ def f2k_sources(text, first_segment=1):
     out = np.zeros(max(1, n.value), T.SOURCE_DTYPE)
     check(lib().ppcb_f2k_sources(b, len(b), int(first_segment), _p(out), len(out), C.byref(n), C.byref(lines)))
     return out[:n.value], lines.value
+
+
+class GradGraph:
+    """The recording forward pass, charge histogram, Poisson weights and log-likelihood and
+    the replay of the detected photons, captured once as a CUDA graph and replayed per call
+    with new ice coefficients (ppcb_gradgraph_*).  Use PPC.gradient_graph to make one."""
+
+    def __init__(self, ctx, bunches, observed, events=0, scale=1.0, hit_cap=None):
+        self._ctx = ctx
+        self._b = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
+        info = ctx.info()
+        self.gsize, self.size, self.events = info["gsize"], info["size"], int(events)
+        self.nbins = self.gsize * (self.events if self.events else 1)
+        obs = np.ascontiguousarray(observed, np.float32).reshape(-1)
+        if obs.size != self.nbins:
+            raise ValueError(f"observed: {obs.size} values for {self.nbins} charge bins")
+        if hit_cap is None:
+            hit_cap = int(self._b["num"].sum() * 0.02) + (1 << 16)
+        self._h = C.c_void_p()
+        check(lib().ppcb_gradgraph_create(ctx._c, _p(self._b), len(self._b), self.events, _p(obs), float(scale),
+                                          int(hit_cap), C.byref(self._h)))
+        ctx._children.add(self)
+
+    def run(self, be=None, ba=None, counts=True):
+        from ._lib import GradInfo
+        b = None if be is None else np.ascontiguousarray(be, np.float32)
+        a = None if ba is None else np.ascontiguousarray(ba, np.float32)
+        cnt = np.zeros(self.nbins, np.uint32) if counts else None
+        g_be = np.zeros(self.size, np.float64)
+        g_ba = np.zeros(self.size, np.float64)
+        gi = GradInfo()
+        check(lib().ppcb_gradgraph_run(self._h, _p(b), _p(a), _p(cnt), _p(g_be), _p(g_ba), C.byref(gi)))
+        if cnt is not None and self.events:
+            cnt = cnt.reshape(self.events, self.gsize)
+        return {"ll": gi.ll, "counts": cnt, "g_be": g_be, "g_ba": g_ba,
+                "info": {k: getattr(gi, k) for k, _ in GradInfo._fields_}}
+
+    def close(self):
+        if self._h:
+            lib().ppcb_gradgraph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def good_list_bad(data, good):

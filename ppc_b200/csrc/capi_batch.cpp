@@ -1,6 +1,7 @@
 // C ABI of the batched launch (declarations: include/ppc_b200.h, "batched events").
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <exception>
 #include <string>
 
@@ -147,6 +148,48 @@ int ppcb_gradient(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t e
       info->backward_ms = r.backward_ms;
     }
   });
+}
+
+struct ppcb_gradgraph {
+  ppcb_ctx* c;
+  std::unique_ptr<ppcb::GradGraph> g;
+};
+
+int ppcb_gradgraph_create(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, uint32_t events, const float* observed,
+                          double scale, uint64_t hit_cap, ppcb_gradgraph** out) {
+  if (!c || !bunches || !observed || !out) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    std::unique_ptr<ppcb_gradgraph> h(new ppcb_gradgraph{c, nullptr});
+    h->g.reset(new ppcb::GradGraph(c->s.eng, bunches, nb, events, observed, scale, hit_cap));
+    *out = h.release();
+  });
+}
+
+int ppcb_gradgraph_run(ppcb_gradgraph* g, const float* be, const float* ba, uint32_t* counts, double* g_be,
+                       double* g_ba, ppcb_grad_info* info) {
+  if (!g) { ppcb_internal_set_error("null argument"); return PPCB_EARG; }
+  return bguard([&] {
+    ppcb::Engine::Grad r = g->g->run(be, ba, counts != nullptr);
+    const int size = g->c->s.eng.cfg.p.size;
+    if (counts) memcpy(counts, r.counts.data(), r.counts.size() * sizeof(uint32_t));
+    if (g_be) memcpy(g_be, r.g_be.data(), size * sizeof(double));
+    if (g_ba) memcpy(g_ba, r.g_ba.data(), size * sizeof(double));
+    if (info) {
+      info->ll = r.ll;
+      info->photons = r.photons;
+      info->hits = r.hits;
+      info->replayed = r.replayed;
+      info->unmatched = r.unmatched;
+      info->steps = r.steps;
+      info->forward_ms = r.forward_ms;
+      info->backward_ms = r.backward_ms;
+    }
+  });
+}
+
+int ppcb_gradgraph_destroy(ppcb_gradgraph* g) {
+  if (!g) return PPCB_OK;
+  return bguard([&] { delete g; });
 }
 
 }  // extern "C"

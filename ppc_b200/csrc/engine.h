@@ -151,4 +151,24 @@ class Engine {
 
 void check(cudaError_t e, const char* what);
 
+// One ice-fit iteration as a CUDA graph (gradient.cu): the recording forward pass, the charge
+// histogram, the Poisson weights and log-likelihood, and the replay of the detected photons
+// over fixed bunches and observed charges, captured once on device 0 and replayed per call
+// with new ice coefficients.  Hit counts stay on the device between the steps.
+struct GradGraphState;
+class GradGraph {
+ public:
+  GradGraph(Engine& e, const ppcb_bunch* b, int nb, uint32_t events, const float* observed, double scale,
+            uint64_t hit_cap);
+  ~GradGraph();
+  // New be/ba (file order; null keeps), then one replay: LL, gradient, charges, timings.
+  Engine::Grad run(const float* be, const float* ba, bool counts = true);
+  GradGraph(const GradGraph&) = delete;
+  GradGraph& operator=(const GradGraph&) = delete;
+
+ private:
+  Engine& e_;
+  std::unique_ptr<GradGraphState> s_;
+};
+
 }  // namespace ppcb

@@ -1130,9 +1130,12 @@ __device__ __forceinline__ long long charge_bin(const ppcb_hit& h, uint32_t even
 // recorded hit is reached again.  A replay that does not end on the recorded hit (same
 // DOM, same time bits) is counted in stats[1].
 __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a, const ppcb_hit* __restrict__ hits,
-                                                 const Prov* __restrict__ prov, uint64_t nh, uint32_t events,
+                                                 const Prov* __restrict__ prov, uint64_t cap,
+                                                 const unsigned long long* nh_dev, uint32_t events,
                                                  const float* __restrict__ wdom, const float2* __restrict__ wgrad,
                                                  double* g_out, unsigned int* stats) {
+  // hits to replay: `cap`, or the recording pass's count from device memory (graph replays)
+  const uint64_t nh = nh_dev ? (*nh_dev < cap ? *nh_dev : cap) : cap;
   __shared__ SmemTables S;
   __shared__ double gbe[PPCB_MAXLYS], gba[PPCB_MAXLYS];
   extern __shared__ __align__(16) unsigned char dsm[];
@@ -1188,20 +1191,19 @@ __global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a
   if (unmatched) atomicAdd(&stats[1], unmatched);
 }
 
-__global__ void k_dom_hist(const ppcb_hit* __restrict__ hits, uint64_t nh, unsigned int* counts, uint32_t events,
-                           int gsize) {
+__global__ void k_dom_hist(const ppcb_hit* __restrict__ hits, uint64_t cap, const unsigned long long* nh_dev,
+                           unsigned int* counts, uint32_t events, int gsize) {
+  const uint64_t nh = nh_dev ? (*nh_dev < cap ? *nh_dev : cap) : cap;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x) {
     const long long b = charge_bin(hits[k], events, gsize);
     if (b >= 0) atomicAdd(&counts[b], 1u);
   }
 }
 
-cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, uint32_t events,
-                           const float* wdom, const float2* wgrad, double* g_out, unsigned int* stats, int blocks,
-                           cudaStream_t st) {
-  if (nh == 0) return cudaSuccess;
-  // its static shared memory plus the string-proximity table exceed the default 48 KiB of
-  // dynamic shared memory: allow the largest table, once per device (before any capture)
+// The replay's static shared memory plus the string-proximity table exceed the default
+// 48 KiB of dynamic shared memory: allow the largest table, once per device (before any
+// stream capture that launches the replay there).
+cudaError_t adjoint_prepare() {
   static std::atomic<uint64_t> done{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -1212,15 +1214,24 @@ cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* pro
     if (e != cudaSuccess) return e;
     done.fetch_or(1ull << (dev & 63));
   }
-  k_adjoint<<<blocks, 256, sg_cells_bytes(a), st>>>(a, hits, static_cast<const Prov*>(prov), nh, events, wdom, wgrad,
-                                                   g_out, stats);
+  return cudaSuccess;
+}
+
+cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, uint32_t events,
+                           const float* wdom, const float2* wgrad, double* g_out, unsigned int* stats, int blocks,
+                           cudaStream_t st, const unsigned long long* nh_dev) {
+  if (nh == 0) return cudaSuccess;
+  const cudaError_t e = adjoint_prepare();
+  if (e != cudaSuccess) return e;
+  k_adjoint<<<blocks, 256, sg_cells_bytes(a), st>>>(a, hits, static_cast<const Prov*>(prov), nh, nh_dev, events,
+                                                   wdom, wgrad, g_out, stats);
   return cudaGetLastError();
 }
 
 cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, uint32_t events, int gsize,
-                            cudaStream_t st) {
+                            cudaStream_t st, const unsigned long long* nh_dev) {
   if (nh == 0) return cudaSuccess;
-  k_dom_hist<<<592, 256, 0, st>>>(hits, nh, counts, events, gsize);
+  k_dom_hist<<<592, 256, 0, st>>>(hits, nh, nh_dev, counts, events, gsize);
   return cudaGetLastError();
 }
 

@@ -67,11 +67,14 @@ cudaError_t launch_index_probe(const KArgs& a, const float4* pos, int n, int32_t
                                cudaStream_t st);
 // Charges are binned per DOM, or with events > 0 per (event, DOM), the event being the
 // hit's segment id (bin = event * gsize + DOM; hits of segments >= events are left out).
+// With nh_dev (a device pointer to the recording pass's hit count) the kernels read how many
+// hits there are at run time, up to nh: a graph replay then needs no host round trip.
 cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* prov, uint64_t nh, uint32_t events,
                            const float* wdom, const float2* wgrad, double* g_out, unsigned int* stats, int blocks,
-                           cudaStream_t st);
+                           cudaStream_t st, const unsigned long long* nh_dev = nullptr);
 cudaError_t launch_dom_hist(const ppcb_hit* hits, uint64_t nh, unsigned int* counts, uint32_t events, int gsize,
-                            cudaStream_t st);
+                            cudaStream_t st, const unsigned long long* nh_dev = nullptr);
+cudaError_t adjoint_prepare();  // the replay's launch attribute on the current device (before a capture)
 constexpr size_t kProvBytes = 64;  // provenance record per hit slot of the gradient's recording pass
 cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size_t* local);
 int propagate_max_blocks_per_sm(int threads);

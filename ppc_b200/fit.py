@@ -89,13 +89,15 @@ def penalty(u, n, smooth, ridge):
 
 
 def fit_ice(ctx, bunches, observed, events, be0=None, ba0=None, iters=20, fit=("be", "ba"), bound=2.0,
-            hit_cap=None, radius=0.05, smooth=0.0, ridge=0.0, callback=None):
+            hit_cap=None, radius=0.05, smooth=0.0, ridge=0.0, callback=None, graph=True):
     """ctx: an initialised PPC (after ini()).  observed: (events, gsize) charges, the event of
     a bunch being its q.  Layers are 10 m thick while a flasher's light samples the ice over
     tens of metres, so neighbouring layers trade off against each other; `smooth` and `ridge`
     add a penalty on layer-to-layer differences and on the distance from the starting ice
-    (in units of log-likelihood per unit of log scale squared).  Returns the fitted be, ba,
-    the LL of every evaluation and timings."""
+    (in units of log-likelihood per unit of log scale squared).  With `graph` each evaluation
+    is one replay of a CUDA graph holding the forward pass and the adjoint
+    (PPC.gradient_graph); otherwise PPC.gradient runs them eagerly.  Returns the fitted be,
+    ba, the LL of every evaluation and timings."""
     if be0 is None or ba0 is None:
         b, a = ctx.get_ice()
         be0 = b if be0 is None else be0
@@ -112,11 +114,16 @@ def fit_ice(ctx, bunches, observed, events, be0=None, ba0=None, iters=20, fit=("
         uba = u[n * use_be:n * use_be + n] if use_ba else np.zeros(n)
         return be0 * np.exp(ube), ba0 * np.exp(uba)
 
+    G = ctx.gradient_graph(bunches, observed, events=events, hit_cap=hit_cap) if graph else None
+
     def fg(u):
         be, ba = unpack(u)
-        ctx.set_ice(be.astype(np.float32), ba.astype(np.float32))
         t0 = time.perf_counter()
-        r = ctx.gradient(bunches, observed=observed, events=events, hit_cap=hit_cap)
+        if G is not None:
+            r = G.run(be.astype(np.float32), ba.astype(np.float32), counts=False)
+        else:
+            ctx.set_ice(be.astype(np.float32), ba.astype(np.float32))
+            r = ctx.gradient(bunches, observed=observed, events=events, hit_cap=hit_cap)
         dt = time.perf_counter() - t0
         g = []
         if use_be:
@@ -137,5 +144,7 @@ def fit_ice(ctx, bunches, observed, events, be0=None, ba0=None, iters=20, fit=("
     wall = time.perf_counter() - t0
     be, ba = unpack(u)
     ctx.set_ice(be.astype(np.float32), ba.astype(np.float32))
+    if G is not None:
+        G.close()
     return {"be": be, "ba": ba, "ll": -f, "history": hist, "iterations": iters, "evaluations": evals,
             "accepted": accepted, "seconds": wall, "seconds_per_iteration": wall / max(1, iters)}

@@ -166,6 +166,32 @@ def test_gradient_matches_per_layer_central_differences(ice_full):
     c.close()
 
 
+def test_gradient_graph_matches_eager_gradient(ice_full):
+    """One fit iteration as a CUDA graph gives what the eager gradient gives, for the starting
+    ice and after new coefficients: the same charges (per-photon streams: the same photons),
+    the log-likelihood and gradient to rounding (sums in another order)."""
+    c = _ctx(ice_full)
+    be0, ba0 = c.get_ice()
+    b = _bunches(c, 20_000_000)
+    b["q"] = [0, 1]
+    gs = c.info()["gsize"]
+    obs = c.gradient(b, weights=np.zeros(2 * gs, np.float32), events=2)["counts"].astype(np.float32) * 1.05
+    G = c.gradient_graph(b, obs, events=2)
+    rng = np.random.default_rng(8)
+    for be, ba in ((be0, ba0), ((be0 * rng.uniform(0.95, 1.05, len(be0))).astype(np.float32),
+                                (ba0 * rng.uniform(0.95, 1.05, len(ba0))).astype(np.float32))):
+        rg = G.run(be, ba)
+        c.set_ice(be, ba)
+        re = c.gradient(b, observed=obs, events=2)
+        assert np.array_equal(rg["counts"], re["counts"])
+        assert abs(rg["ll"] - re["ll"]) <= 1e-9 * abs(re["ll"])
+        for k in ("g_be", "g_ba"):
+            assert np.allclose(rg[k], re[k], rtol=1e-9, atol=1e-9 * np.abs(re[k]).max()), k
+        assert rg["info"]["hits"] == re["info"]["hits"] and rg["info"]["replayed"] == re["info"]["replayed"]
+    G.close()
+    c.close()
+
+
 def test_likelihood_weights(ice_full):
     """observed counts -> LL = sum k log mu - mu and w_d = k_d/mu_d - 1, the gradient equal
     to the one with those weights given explicitly."""
