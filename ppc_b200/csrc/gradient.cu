@@ -305,6 +305,7 @@ GradGraph::GradGraph(Engine& e, const ppcb_bunch* b, int nb, uint32_t events, co
   const unsigned long long* nh_dev = &S.ctrl.p->hidx;
   check(adjoint_prepare(), "replay attribute");
 
+  // the timing events are recorded as external event nodes, so that a replay records them
   check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
   cudaError_t err = cudaSuccess;
   auto q = [&](cudaError_t x) { if (err == cudaSuccess) err = x; };
@@ -313,9 +314,9 @@ GradGraph::GradGraph(Engine& e, const ppcb_bunch* b, int nb, uint32_t events, co
   q(cudaMemsetAsync(S.counts.p, 0, S.nbins * sizeof(unsigned int), st));
   q(cudaMemsetAsync(S.g.p, 0, 2 * PPCB_MAXLYS * sizeof(double), st));
   q(cudaMemsetAsync(S.stats.p, 0, 2 * sizeof(unsigned int), st));
-  q(cudaEventRecord(S.ev[0], st));
+  q(cudaEventRecordWithFlags(S.ev[0], st, cudaEventRecordExternal));
   q(launch_propagate(a, shape, st));
-  q(cudaEventRecord(S.ev[1], st));
+  q(cudaEventRecordWithFlags(S.ev[1], st, cudaEventRecordExternal));
   q(launch_dom_hist(S.hits.p, hit_cap, S.counts.p, events, e.cfg.p.gsize, st, nh_dev));
   k_weights<<<kWBlocks, kWThreads, 0, st>>>(S.counts.p, S.observed.p, S.nbins, scale, S.weights.p, S.part.p);
   q(cudaGetLastError());
@@ -323,7 +324,7 @@ GradGraph::GradGraph(Engine& e, const ppcb_bunch* b, int nb, uint32_t events, co
   q(cudaGetLastError());
   q(launch_adjoint(r, S.hits.p, S.prov.p, hit_cap, events, S.weights.p, S.wgrad.p, S.g.p, S.stats.p,
                    g.prop.multiProcessorCount * 4, st, nh_dev));
-  q(cudaEventRecord(S.ev[2], st));
+  q(cudaEventRecordWithFlags(S.ev[2], st, cudaEventRecordExternal));
   q(cudaMemcpyAsync(S.hg.p, S.g.p, 2 * PPCB_MAXLYS * sizeof(double), cudaMemcpyDeviceToHost, st));
   q(cudaMemcpyAsync(S.hll.p, S.ll.p, sizeof(double), cudaMemcpyDeviceToHost, st));
   q(cudaMemcpyAsync(S.hstats.p, S.stats.p, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
