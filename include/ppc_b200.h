@@ -250,8 +250,9 @@ int ppcb_gradgraph_destroy(ppcb_gradgraph* g);
  * clamped to the sum on the device.  The call allocates nothing; the context's tables come
  * from an earlier ppcb_ini.  The caller's current device is left as it was.
  * Each call looks up the array's device address with the device current (a host-side
- * lookup, no allocation); the first call on a device may load the library's device code,
- * so make that first call before any stream capture.  All calls on a device share the one
+ * lookup, no allocation); the first call on a device may also load the library's device
+ * code (the runtime's module loading, not an allocation by this library).  All calls on a
+ * device share the one
  * array and it keeps the last call's contents (each call clears its counters first): calls
  * whose work overlaps on the GPU race, so order them (one stream, or events). */
 #define PPCB_NOALLOC_MAX_BUNCHES 65536
@@ -320,7 +321,10 @@ int ppcb_f2k_sources(const char* text, uint64_t len, uint32_t first_segment, ppc
  * every simulated hit by +dt.  Simulated hits count 1 each (DirectFit without SPE charge
  * sampling).  As in the reference, with norm a DOM that enters with all of its observed
  * charge outside the 200 bins (dtot = 0) makes the result NaN.
- * Not supported: the "good DOM" list, multi-PMT keys, the charge-unfolding variants. */
+ * A good-DOM list (DirectFit's `set` file) enters as bad DOMs: those with observed pulses
+ * that are not on it, which is what llh/llh.cxx:785-792 does with it; `unh` stays the
+ * caller's choice, as the list does not set it there.
+ * Not supported: multi-PMT keys, the charge-unfolding variants. */
 typedef struct ppcb_llh ppcb_llh;
 typedef struct ppcb_llh_hit {        /* one observed pulse: the columns of DirectFit's dat file */
   int32_t str, om;

@@ -1,4 +1,5 @@
-"""Parity with the reference at the north star's tolerance, against high-statistics
+"""Statistical parity with the reference (totals within 0.1%, per-DOM counts within 3
+sigma, hit-time KS p > 0.01), against high-statistics
 fixtures made by the reference's own CPU build (tests/golden/make_parity_fixture.py:
 gpu/ppc.cu + gpu/pro.cu compiled with its --fast-math flags, thousands of seeds).
 
