@@ -25,6 +25,13 @@ static ppco_counts g_cnt;
 void ppco_counts_reset(void) { memset(&g_cnt, 0, sizeof(g_cnt)); }
 void ppco_counts_get(ppco_counts* out) { *out = g_cnt; }
 
+/* Optional step trace: the segment each step hands to the DOM search (position, direction,
+ * geometric length), 8 floats per step, in the layout ppco_string_pass reads. */
+static float* g_trace;
+static uint64_t g_trace_cap, g_trace_n;
+void ppco_trace_steps(float* buf, uint64_t cap) { g_trace = buf; g_trace_cap = cap; g_trace_n = 0; }
+uint64_t ppco_trace_count(void) { return g_trace_n; }
+
 /* std::min / std::max argument-order semantics */
 static inline float mnf(float a, float b) { return b < a ? b : a; }
 static inline float mxf(float a, float b) { return a < b ? b : a; }
@@ -428,6 +435,10 @@ uint64_t ppco_propagate(const ppco_tables* t, const ppco_pbuf* f, ppco_rng* s, p
     om = -1;
     float del = sca;
     float hi = sca, hf = 0;
+    if (g_trace && g_trace_n < g_trace_cap) {
+      float* q = g_trace + 8 * g_trace_n++;
+      q[0] = r.x; q[1] = r.y; q[2] = r.z; q[3] = r.w; q[4] = n.x; q[5] = n.y; q[6] = n.z; q[7] = sca;
+    }
     {  /* DOM search through the cell grid, gpu/pro.cu:577-672 */
       int xlx, xhx, xly, xhy;
       cell_range(e, r.x, r.y, r.x + sca * n.x, r.y + sca * n.y, &xlx, &xhx, &xly, &xhy);

@@ -42,6 +42,9 @@ typedef struct ppco_counts {
 } ppco_counts;
 void ppco_counts_reset(void);
 void ppco_counts_get(ppco_counts* out);
+/* step trace: each step's DOM-search segment (r.xyzw, n.xyz, sca), at most cap steps */
+void ppco_trace_steps(float* buf, uint64_t cap);
+uint64_t ppco_trace_count(void);
 
 /* phase-1 photon record (gpu/ini.cxx:391-397) */
 typedef struct ppco_pbuf {

@@ -1083,7 +1083,8 @@ void Config::build_strgrid() {
     }
     if (!merged) sg_groups.push_back(StrGroup{sc[m].x, sc[m].y, sc[m].r + kReachPad, 0});
   }
-  if (sg_groups.size() >= kSgNone) throw Error("string-proximity table: too many string axes");
+  if (sg_groups.size() >= 255) throw Error("string-proximity table: too many string axes");
+  const int ng = (int)sg_groups.size();
   const double margin = 64;
   double x0 = 1e30, x1 = -1e30, y0 = 1e30, y1 = -1e30;
   for (auto& g : sg_groups) {
@@ -1098,18 +1099,19 @@ void Config::build_strgrid() {
     if ((long)nx * ny <= kSgMaxCells) break;
     cell *= 1.25;
   }
-  sg.ox = (float)(x0 - margin);
-  sg.oy = (float)(y0 - margin);
+  const double ox = x0 - margin, oy = y0 - margin;
   sg.inv = (float)(1 / cell);
-  sg.margin = (float)margin;
+  sg.ou = (float)(-ox / cell);
+  sg.ov = (float)(-oy / cell);
+  sg.margin2 = (float)(margin * margin);
   sg.nx = nx; sg.ny = ny; sg.on = 1;
   sg_cells.assign((size_t)nx * ny, 0);
-  const int ng = (int)sg_groups.size();
   for (int j = 0; j < ny; j++)
     for (int i = 0; i < nx; i++) {
-      // the cell as the device indexes it, widened by a micrometre on each side
-      const double xa = sg.ox + i * cell - 1e-6, xb = sg.ox + (i + 1) * cell + 1e-6;
-      const double ya = sg.oy + j * cell - 1e-6, yb = sg.oy + (j + 1) * cell + 1e-6;
+      // the cell of the device's index arithmetic, widened by a millimetre on each side
+      // (the index is computed in single precision from the origin and the cell size)
+      const double xa = ox + i * cell - 1e-3, xb = ox + (i + 1) * cell + 1e-3;
+      const double ya = oy + j * cell - 1e-3, yb = oy + (j + 1) * cell + 1e-3;
       int best = -1;
       double d1 = 1e30, d2 = 1e30;  // nearest and second-nearest disc distance
       for (int k = 0; k < ng; k++) {
@@ -1121,8 +1123,9 @@ void Config::build_strgrid() {
       }
       const double q = std::floor(d2 / kSgClearUnit);
       const unsigned int clear = q > 255 ? 255u : (unsigned int)q;
-      sg_cells[(size_t)j * nx + i] = (uint16_t)((clear << 8) | (unsigned int)(best < 0 ? kSgNone : best));
+      sg_cells[(size_t)j * nx + i] = (uint16_t)((clear << 8) | (unsigned int)(best < 0 ? ng : best));
     }
+  sg_groups.push_back(StrGroup{1e30f, 1e30f, 0, 0});  // the sentinel: no group within reach
 }
 
 }  // namespace ppcb

@@ -46,7 +46,7 @@ struct SmemTables {
   uint16_t is[PPCB_CX * PPCB_CY];
   int8_t mcol[PPCB_CTX * PPCB_CTY];
   float4 bfrt[PPCB_BFR_TAB + 1];  // birefringence angular functions (sx, sy, mx, -)
-  StrGroup sgg[PPCB_NSTR];        // string-proximity table: string axes (strgrid.h)
+  StrGroup sgg[PPCB_NSTR + 1];    // string-proximity table: string axes and the sentinel (strgrid.h)
   float4 azr[PPCB_MAXLYS];        // per layer 1/k1, 1/k2, 1/(k1 k2): the scattering's frame divisions
 };
 

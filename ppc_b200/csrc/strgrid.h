@@ -17,8 +17,9 @@
 //
 // A step from r, of length sca along n, reaches horizontally no farther than
 // L = sca sqrt(1 - nz^2) from r.  If L is below the cell's clearance no other group can be
-// reached, and the nearest one is tested with the reference's cylinder arithmetic on the
-// widened radius.  A string that the reference's test accepts is within its radius of the
+// reached.  The nearest group is then out of reach when r lies farther than rw + sca from
+// its axis (a ball test, no square root); otherwise it is tested with the reference's
+// cylinder arithmetic on the widened radius.  A string that the reference's test accepts is within its radius of the
 // segment, so the widened test accepts it too: the widening changes the test's
 // discriminant by 0.09 np m^2, against a rounding of at most 1e-3 np m^2 for strings
 // within 120 m of the segment.  When nothing can be reached the reference's search would
@@ -45,17 +46,19 @@ constexpr float kReachPad = 0.05f;      // [m] added to every group's radius
 constexpr float kSgClearUnit = 0.5f;    // [m] clearance quantum of a cell entry (8 bits)
 constexpr int kSgMaxCells = 16384;      // cells (two bytes each): 32 KiB of shared memory
 constexpr float kSgMinNp = 1e-4f;       // 1 - nz^2 below this: full search
-constexpr uint32_t kSgNone = 0xff;      // cell entry: no group
 
-// Table geometry (a kernel parameter).  Cell (i, j) covers
-// [ox + i cell, ox + (i+1) cell) x [oy + j cell, oy + (j+1) cell).  A point outside the
-// grid is at least `margin` from every group's widened disc.
+// Table geometry (a kernel parameter).  Point (x, y) lies in cell
+// (floor(x inv + ou), floor(y inv + ov)), whose square on the host is widened by a
+// millimetre on every side to cover the rounding of that product.  A point outside the
+// grid is at least sqrt(margin2) from every group's widened disc.
 struct StrGridParams {
-  float ox, oy, inv, margin;  // origin, 1 / cell size, distance bound outside the grid
-  int32_t nx, ny, on, pad_;   // cells per row, rows; on = 0: no strings (nothing to search)
+  float ou, ov, inv, margin2;  // -origin / cell size, 1 / cell size, squared distance bound outside the grid
+  int32_t nx, ny, on, pad_;    // cells per row, rows; on = 0: no strings (nothing to search)
 };
 
-// One group as the pre-test reads it: axis and widened radius.
+// One group as the pre-test reads it: axis and widened radius.  After the groups the
+// table holds a sentinel (an axis at 1e30 m, never within reach), the entry of a cell
+// that has no nearest group.
 struct StrGroup {
   float x, y, rw, pad_;
 };
@@ -75,7 +78,7 @@ PPCB_SG_HD bool sg_group_near(const StrGroup& G, float rx, float ry, float nx, f
 
 // Whether the step may reach a string's cylinder (the full search must run).  `Tab`
 // supplies cell(k) (the 16-bit cell entry: group in the low byte, clearance in the high
-// byte) and group(m).
+// byte) and group(m).  Host and device evaluate it with the same IEEE operations.
 template <class Tab>
 PPCB_SG_HD bool sg_may_reach(const StrGridParams& g, const Tab& t, float rx, float ry, float nx, float ny, float nz,
                              float sca) {
@@ -87,14 +90,21 @@ PPCB_SG_HD bool sg_may_reach(const StrGridParams& g, const Tab& t, float rx, flo
   const float np = 1 - nz * nz;
   if (!(np >= kSgMinNp)) return true;
   const float L2 = sca * sca * np;  // squared horizontal reach of the step
-  const float u = (rx - g.ox) * g.inv, v = (ry - g.oy) * g.inv;
-  if (!(u >= 0 && v >= 0 && u < (float)g.nx && v < (float)g.ny))  // outside the grid (or NaN)
-    return !(L2 < g.margin * g.margin);
-  const uint32_t e = t.cell((int)v * g.nx + (int)u);
+#if defined(__CUDA_ARCH__)
+  const int iu = __float2int_rd(fmaf(rx, g.inv, g.ou)), iv = __float2int_rd(fmaf(ry, g.inv, g.ov));
+#else
+  const float fu = std::floor(std::fma(rx, g.inv, g.ou)), fv = std::floor(std::fma(ry, g.inv, g.ov));
+  const int iu = fu >= 0 && fu < (float)g.nx ? (int)fu : -1, iv = fv >= 0 && fv < (float)g.ny ? (int)fv : -1;
+#endif
+  if (!((unsigned)iu < (unsigned)g.nx && (unsigned)iv < (unsigned)g.ny))  // outside the grid (or NaN)
+    return !(L2 < g.margin2);
+  const uint32_t e = t.cell(iv * g.nx + iu);
   const float clear = (float)(e >> 8) * kSgClearUnit;
   if (!(L2 < clear * clear)) return true;  // another group may be within reach
-  const uint32_t m = e & 0xff;
-  return m != kSgNone && sg_group_near(t.group((int)m), rx, ry, nx, ny, np, sca);
+  const StrGroup& G = t.group((int)(e & 0xff));
+  const float dx = G.x - rx, dy = G.y - ry, w = G.rw + sca;
+  if (dx * dx + dy * dy > w * w) return false;  // the nearest axis is farther than rw + sca
+  return sg_group_near(G, rx, ry, nx, ny, np, sca);
 }
 
 }  // namespace ppcb
