@@ -4,8 +4,8 @@
 // strings of the skewed search cells (about 62 m wide) that the step's horizontal extent
 // touches and tests each string's cylinder against the step's segment.  On the full
 // detector that is about two strings per step, while fewer than 0.2% of steps pass a
-// cylinder test at all.  This table lets a step prove, with one shared-memory load and one
-// cylinder test, that the search would find nothing:
+// cylinder test at all.  This table lets a step prove, with one shared-memory load and a
+// distance test (a cylinder test near a string), that the search would find nothing:
 //
 //   * lines that share an axis (a string split into several lines, axes equal up to
 //     rounding) form a group, whose disc covers each line's search disc (the search radius
