@@ -210,7 +210,8 @@ def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps
                  2-d tilt detector with cables; CPU: the reference's own print() (one core)
       likelihood ppcb_llh_eval_device, DirectFit's likelihood of those hits against the pulses
                  of a 1e7-photon run of the same cascade, 64 time shifts per evaluation; CPU:
-                 the oracle's restatement (the reference's llh.cxx needs GSL), one core
+                 the oracle's restatement (pinned bit for bit to the reference's llh.cxx,
+                 which runs here only against a GSL stand-in), one core
       front end  ppcb_sources_device over 1e6 mixed sources (muon segments, EM and hadronic
                  cascades, 0.1-10 GeV); CPU: the reference's own addp() (one core)"""
     import torch
@@ -301,8 +302,8 @@ def stages_sample(local, photons=100_000_000, sources=1_000_000, shifts=64, reps
         O.llh_fllh(data, sim, dts[:8], 10.0)
         secs = time.perf_counter() - t0
         lk["cpu"] = {"evals_per_s": 8 / secs, "cores": 1, "kind": "port",
-                     "sample": "8 shifts of the same evaluation through oracle/llh_oracle.c (DirectFit's "
-                               "llh.cxx needs GSL, absent here), accepted hits given"}
+                     "sample": "8 shifts of the same evaluation through oracle/llh_oracle.c (equal bit for "
+                               "bit to DirectFit's llh.cxx on its golden vectors), accepted hits given"}
         lk["speedup_vs_cpu"] = lk["evals_per_s"] / lk["cpu"]["evals_per_s"]
     except Exception as e:  # the oracle library is a build product of oracle/Makefile
         lk["cpu"] = {"unavailable": str(e)[:120]}

@@ -15,6 +15,9 @@
 //     in shared memory; the per-wavelength ice table, tilt maps and DOMs are read
 //     through the read-only cache from HBM (they are L2-resident: < 1 MB);
 //   * hits are appended with one atomic per coalesced group of hitting lanes;
+//   * paired components ((x, y) of a direction, (absorption, scattering) of a layer) go
+//     through sm_100's two-lane FP32 instructions (__ffma2_rn and the like), one issue slot
+//     for two operations in a kernel whose limit is instruction issue;
 //   * the index helpers (tilt shift, layer, cell range, DOM window) use explicit
 //     round-to-nearest operations without contraction, so for identical positions they
 //     are bit-identical to the IEEE CPU restatement; the rest of the physics uses the
@@ -707,8 +710,9 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
   float nr = 1.f;
   {
     if (TOT > 0) {  // absorption anisotropy, gpu/pro.cu:517-544
-      float n1 = e.azx * n.x + e.azy * n.y;
-      float n2 = -e.azy * n.x + e.azx * n.y;
+      float2 n12 = __ffma2_rn(make_float2(e.azx, -e.azy), make_float2(n.x, n.x),
+                              __fmul2_rn(make_float2(e.azy, e.azx), make_float2(n.y, n.y)));
+      float n1 = n12.x, n2 = n12.y;
       float n3 = n.z;
       if (e.fr != 0) {
         float k1 = S.az[I].k1, k2 = S.az[I].k2;
@@ -721,30 +725,33 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
         float An = s1 * l1 + s2 * l2 + s3 * l3;
         nr = powf((B2 - nB) * An / 2, e.fr);
       }
-      n1 *= e.k1; n2 *= e.k2; n3 *= e.kz;
+      n12 = __fmul2_rn(n12, make_float2(e.k1, e.k2));
+      n1 = n12.x; n2 = n12.y; n3 *= e.kz;
       nr *= rsqrtf(n1 * n1 + n2 * n2 + n3 * n3);
       TOT /= nr;
     }
     float ahx = edh * (0.5f - sign * (z - I));
     J = I;  // layer stepping, gpu/pro.cu:548-571
-    sca = 0; tot = 0;
-    float ais = SCA, aia = TOT;
+    // (absorption, scattering) pairs in two-lane FP32 operations, as the table stores them
+    float2 ts = make_float2(0.f, 0.f);   // (tot, sca)
+    float2 aa = make_float2(TOT, SCA);   // (aia, ais)
     float2 c = ice(wz, J);
     while (true) {
-      float dsca = ais / c.y, dtot = aia / c.x;
+      float dsca = aa.y / c.y, dtot = aa.x / c.x;
       float dist = fminf(dsca, dtot) * anz;
       if ((sign < 0 ? J > 0 : J < e.size - 1) && dist > ahx) {
         float del = ahx / anz;
-        sca += del; tot += del;
-        ais -= c.y * del; aia -= c.x * del;
+        ts = __fadd2_rn(ts, make_float2(del, del));
+        aa = __ffma2_rn(c, make_float2(-del, -del), aa);
         ahx = edh;
         J += sign;
         c = ice(wz, J);
       } else {
-        sca += dsca; tot += dtot;
+        ts = __fadd2_rn(ts, make_float2(dtot, dsca));
         break;
       }
     }
+    tot = ts.x; sca = ts.y;
     if (sca < 0) sca = 0;
     if (tot < 0) tot = 0;
     if (tot < sca) { sca = tot; tot = 0; }
@@ -770,7 +777,12 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
   } else { SCA = 0; TOT = tot * nr; }
 
   hk.segment(I, z, sign, anz, edh, nr, fin, n.z, e.size);  // bulk-ice part of the step (the rest is hole ice)
-  r.x += del * n.x; r.y += del * n.y; r.z += del * n.z; r.w += del * n.w;
+  {
+    const float2 d2 = make_float2(del, del);
+    const float2 rxy = __ffma2_rn(d2, make_float2(n.x, n.y), make_float2(r.x, r.y));
+    const float2 rzw = __ffma2_rn(d2, make_float2(n.z, n.w), make_float2(r.z, r.w));
+    r = make_float4(rxy.x, rxy.y, rzw.x, rzw.y);
+  }
 
   if (!isfinite(TOT) || !isfinite(SCA)) {  // gpu/pro.cu:728
     record_nan_step(a);
@@ -805,58 +817,67 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
       }
       if (ra < 0) ra = 0;
       if (rb < 0) rb = 0;
+      // The (x, y) components go through the two-lane FP32 operations (__ffma2_rn,
+      // __fmul2_rn, __fadd2_rn: one instruction for two operations), the z component alone.
+      const float2 nxy = make_float2(n.x, n.y);
       float dot = e.azx * n.x + e.azy * n.y;
       // angular diffusion functions of gpu/pro.cu:784-786, tabulated on the host in
       // v = sqrt(1 - |dot|) (smooth in v at both ends) and interpolated linearly
-      float sx, sy, mx;
+      float2 sxy;
+      float mx;
       {
         const float v = sqrtf(fmaxf(0.f, 1.f - fabsf(dot))) * PPCB_BFR_TAB;
         const int iv = min((int)v, PPCB_BFR_TAB - 1);
         const float fv = v - iv;
         const float4 t0 = S.bfrt[iv], t1 = S.bfrt[iv + 1];
         const float sra = sqrtf(ra);
-        sx = sra * fmaf(fv, t1.x - t0.x, t0.x);
-        sy = sra * fmaf(fv, t1.y - t0.y, t0.y);
+        const float2 a0 = make_float2(t0.x, t0.y);
+        const float2 d01 = __fadd2_rn(make_float2(t1.x, t1.y), make_float2(-t0.x, -t0.y));
+        sxy = __fmul2_rn(make_float2(sra, sra), __ffma2_rn(make_float2(fv, fv), d01, a0));
         mx = rb * fmaf(fv, t1.z - t0.z, t0.z);
       }
-      float qx = e.azx - dot * n.x, qy = e.azy - dot * n.y, qz = -dot * n.z;
-      if (dot < 0) { qx = -qx; qy = -qy; qz = -qz; }
-      float qn = qx * qx + qy * qy + qz * qz;
+      const float sg = dot < 0 ? -1.f : 1.f;
+      float2 qxy = __fmul2_rn(__ffma2_rn(make_float2(-dot, -dot), nxy, make_float2(e.azx, e.azy)), make_float2(sg, sg));
+      float qz = -dot * n.z * sg;
+      float qn = qxy.x * qxy.x + qxy.y * qxy.y + qz * qz;
       if (qn > 0) {
         float f = rsqrtf(qn);
-        qx *= f; qy *= f; qz *= f;
-      } else { qx = 0; qy = 0; qz = 1; }
-      float px = n.y * qz - n.z * qy, py = n.z * qx - n.x * qz, pz = n.x * qy - n.y * qx;
+        qxy = __fmul2_rn(qxy, make_float2(f, f)); qz *= f;
+      } else { qxy = make_float2(0.f, 0.f); qz = 1; }
+      const float2 pxy = __ffma2_rn(make_float2(n.y, n.z), make_float2(qz, qxy.x),
+                                    __fmul2_rn(make_float2(-n.z, -n.x), make_float2(qxy.y, qz)));
+      const float pz = n.x * qxy.y - n.y * qxy.x;
       float2 rnd = grnd2(s);
-      float dnx = sx * rnd.x + mx;
-      float dny = sy * rnd.y;
+      float2 dn = __ffma2_rn(sxy, rnd, make_float2(mx, 0.f));
       if (del <= hi) {  // curved path within the segment
         rnd = grnd2(s);
-        float vnx = dnx + sx * rnd.x * rsqrtf(3.f);
-        float vny = dny + sy * rnd.y * rsqrtf(3.f);
-        vnx /= 2; vny /= 2;
-        float den = vnx * vnx + vny * vny;
+        float2 vn = __fmul2_rn(__ffma2_rn(__fmul2_rn(sxy, rnd), make_float2(rsqrtf(3.f), rsqrtf(3.f)), dn),
+                               make_float2(0.5f, 0.5f));
+        float den = vn.x * vn.x + vn.y * vn.y;
         float dnz = -den;
         den = 2 / (1 + den);
-        vnx *= den; vny *= den; dnz *= den;
+        vn = __fmul2_rn(vn, make_float2(den, den)); dnz *= den;
+        float2 mxy = __ffma2_rn(nxy, make_float2(dnz, dnz),
+                                __ffma2_rn(pxy, make_float2(vn.y, vn.y), __ffma2_rn(qxy, make_float2(vn.x, vn.x), nxy)));
         float4 m;
-        m.x = n.x + qx * vnx + px * vny + n.x * dnz;
-        m.y = n.y + qy * vnx + py * vny + n.y * dnz;
-        m.z = n.z + qz * vnx + pz * vny + n.z * dnz;
+        m.x = mxy.x; m.y = mxy.y;
+        m.z = n.z + qz * vn.x + pz * vn.y + n.z * dnz;
         normalize3(m);
         del -= fin / 2;
-        r.x += del * (m.x - n.x);
-        r.y += del * (m.y - n.y);
+        const float2 rxy = __ffma2_rn(make_float2(del, del), __fadd2_rn(make_float2(m.x, m.y), make_float2(-n.x, -n.y)),
+                                      make_float2(r.x, r.y));
+        r.x = rxy.x; r.y = rxy.y;
         r.z += del * (m.z - n.z);
       }
-      dnx /= 2; dny /= 2;
-      float den = dnx * dnx + dny * dny;
+      dn = __fmul2_rn(dn, make_float2(0.5f, 0.5f));
+      float den = dn.x * dn.x + dn.y * dn.y;
       float dnz = -den;
       den = 2 / (1 + den);
-      dnx *= den; dny *= den; dnz *= den;
-      n.x += qx * dnx + px * dny + n.x * dnz;
-      n.y += qy * dnx + py * dny + n.y * dnz;
-      n.z += qz * dnx + pz * dny + n.z * dnz;
+      dn = __fmul2_rn(dn, make_float2(den, den)); dnz *= den;
+      const float2 nn = __ffma2_rn(nxy, make_float2(dnz, dnz),
+                                   __ffma2_rn(pxy, make_float2(dn.y, dn.y), __ffma2_rn(qxy, make_float2(dn.x, dn.x), nxy)));
+      n.z += qz * dn.x + pz * dn.y + n.z * dnz;
+      n.x = nn.x; n.y = nn.y;
       normalize3(n);
     }
     if (SCA < XXX) {  // scattering, gpu/pro.cu:838-887
@@ -1129,7 +1150,7 @@ __device__ __forceinline__ long long charge_bin(const ppcb_hit& h, uint32_t even
 // the path's per-layer derivative terms, weighted by the hit's DOM weight, until the
 // recorded hit is reached again.  A replay that does not end on the recorded hit (same
 // DOM, same time bits) is counted in stats[1].
-__global__ void __launch_bounds__(256) k_adjoint(const __grid_constant__ KArgs a, const ppcb_hit* __restrict__ hits,
+__global__ void __launch_bounds__(256, 3) k_adjoint(const __grid_constant__ KArgs a, const ppcb_hit* __restrict__ hits,
                                                  const Prov* __restrict__ prov, uint64_t cap,
                                                  const unsigned long long* nh_dev, uint32_t events,
                                                  const float* __restrict__ wdom, const float2* __restrict__ wgrad,
