@@ -127,9 +127,7 @@ __device__ __forceinline__ float2 grnd2(Rng& s) {
   float r = sqrtf(-2 * logf(xrnd(s)));
   float2 p;
   sincosf(2 * FPI * xrnd(s), &p.y, &p.x);
-  p.x *= r;
-  p.y *= r;
-  return p;
+  return __fmul2_rn(p, make_float2(r, r));
 }
 
 __device__ __forceinline__ void swp(float& a, float& b) { float t = a; a = b; b = t; }
@@ -804,7 +802,10 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
   else {
     if (e.sum > 0 && fin > 0) {  // birefringence diffusion, gpu/pro.cu:757-836
       float ra, rb;
-      if (I == J) { ra = fin * S.az[I].ra; rb = fin * S.az[I].rb; }
+      if (I == J) {
+        const float2 q = __fmul2_rn(make_float2(fin, fin), make_float2(S.az[I].ra, S.az[I].rb));
+        ra = q.x; rb = q.y;
+      }
       else {
         float y = z + n.z * fin / edh;
         float h = 0.5f - sign * (z - I);
