@@ -51,6 +51,7 @@ struct SmemTables {
   float4 bfrt[PPCB_BFR_TAB + 1];  // birefringence angular functions (sx, sy, mx, -)
   StrGroup sgg[PPCB_NSTR + 1];    // string-proximity table: string axes and the sentinel (strgrid.h)
   float4 azr[PPCB_MAXLYS];        // per layer 1/k1, 1/k2, 1/(k1 k2): the scattering's frame divisions
+  float4 scat[2][2];              // bulk [0] / hole ice [1]: (sf, g, gr, 1/(1-sf)), (1-g^2, (1-g)^2, 1/(2g), 1/sf)
 };
 
 // ---------------------------------------------------------------- IEEE helpers
@@ -884,20 +885,18 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
     if (SCA < XXX) {  // scattering, gpu/pro.cu:838-887
       if (!hole) hk.scatter(J, ice(wz, J).y);
       SCA = 0;
-      float sf, g, gr;
-      if (hole) { sf = e.SF; g = e.G; gr = e.GR; }
-      else { sf = e.sf; g = e.g; gr = e.gr; }
+      const float4 c0 = S.scat[hole][0], c1 = S.scat[hole][1];
       float xi = xrnd(s);
-      if (xi > sf) {
-        xi = (1 - xi) / (1 - sf);
+      if (xi > c0.x) {
+        xi = (1 - xi) * c0.w;
         xi = 2 * xi - 1;
-        if (g != 0) {
-          float ga = (1 - g * g) / (1 + g * xi);
-          xi = (ga * ga - (1 - g) * (1 - g)) / (2 * g);
+        if (c0.y != 0) {
+          float ga = c1.x / (1 + c0.y * xi);
+          xi = (ga * ga - c1.y) * c1.z;
         }
       } else {
-        xi /= sf;
-        xi = 2 * (1 - powf(xi, gr));
+        xi *= c1.w;
+        xi = 2 * (1 - powf(xi, c0.z));
       }
       if (xi < 0) xi = 0;
       else if (xi > 2) xi = 2;
@@ -935,6 +934,12 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
   for (int i = t; i < PPCB_CTX * PPCB_CTY; i += nt) S.mcol[i] = a.mcol[i];
   for (int i = t; i <= PPCB_BFR_TAB; i += nt) S.bfrt[i] = a.bfrt[i];
   for (int i = t; i < a.sg_ngroups; i += nt) S.sgg[i] = a.sg_groups[i];
+  if (t < 2) {
+    const float sf = t ? a.p.SF : a.p.sf, g = t ? a.p.G : a.p.g, gr = t ? a.p.GR : a.p.gr;
+    S.scat[t][0] = make_float4(sf, g, gr, __fdiv_rn(1.f, __fsub_rn(1.f, sf)));
+    S.scat[t][1] = make_float4(__fsub_rn(1.f, __fmul_rn(g, g)), __fmul_rn(__fsub_rn(1.f, g), __fsub_rn(1.f, g)),
+                               __fdiv_rn(1.f, __fmul_rn(2.f, g)), __fdiv_rn(1.f, sf));
+  }
   for (int i = t; i < a.p.size; i += nt) {
     const ppcb_aniz z = a.az[i];
     S.azr[i] = make_float4(__fdividef(1.f, z.k1), __fdividef(1.f, z.k2), __fdividef(1.f, z.k1 * z.k2), 0.f);
