@@ -44,7 +44,8 @@ class PPC:
     def set_options(self, deterministic=False, max_steps=1_000_000, blocks_per_sm=0, photon_streams=False):
         """deterministic: photon i on thread i mod T (the reference's order).  photon_streams:
         each photon draws from its own stream keyed by (seed, i), whatever thread runs it, so
-        runs that differ only in the ice share every photon's random numbers."""
+        runs that differ only in the ice share every photon's random numbers.  i counts the
+        photons of one launch: launches that should be independent need different seeds."""
         mode = 2 if photon_streams else int(bool(deterministic))
         check(lib().ppcb_set_options(self._c, mode, int(max_steps), int(blocks_per_sm)))
 
