@@ -833,7 +833,8 @@ def run_ours(args, rank, world, local):
 
     # end to end through the host API: bunch upload, launch, hit download; the timed
     # iterations replay the cascades of the device-timed steps
-    e2e_times, e2e_hits = [], 0
+    e2e_times, e2e_hits, e2e_dev_ms = [], 0, 0.0
+    clk_e2e = Clocks(local) if (rank == 0 and not args.no_e2e) else None
     for k in range(0 if args.no_e2e else args.warmup + args.steps):
         if k < args.warmup:
             b = _cascade_bunch(rng, photons, q=1, ppm=ppm, fixed=args.cascade)[0]
@@ -848,6 +849,8 @@ def run_ours(args, rank, world, local):
         if k >= args.warmup:
             e2e_times.append(t1 - t0)
             e2e_hits += len(h)
+            e2e_dev_ms += inf["device_ms"]
+    e2e_clocks = clk_e2e.stop() if clk_e2e else None
     e2e_total = max_over_ranks(sum(e2e_times) if e2e_times else float("nan"))
 
     if rank != 0:
@@ -908,7 +911,12 @@ def run_ours(args, rank, world, local):
         "hits_per_step": hits / args.steps,
         "gpu_launches": args.steps,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": int(d2h), "gpu_launches": args.steps},
+                "d2h_bytes_per_step": int(d2h), "gpu_launches": args.steps,
+                # where the end-to-end time went: the library's own launch timing (CUDA events
+                # around upload, kernel and control read-back) against the wall clock
+                "wall_ms_per_step": 1e3 * sum(e2e_times) / max(1, len(e2e_times)),
+                "device_ms_per_step": e2e_dev_ms / max(1, len(e2e_times)),
+                "clocks": e2e_clocks},
         "roofline": roofline,
         "clocks": clocks,
     }
