@@ -118,16 +118,26 @@ __device__ float mrnd(float k, Rng& s) {
   return x;
 }
 
+// 2 pi xrnd(s) as one FMA on the generator's [1, 2) float f: xrnd = 2 - f exactly (Sterbenz),
+// and 4 pi, 2 pi differ by a power of two, so the product 2 pi (2 - f) rounds the same way.
+__device__ __forceinline__ float xrnd_angle(Rng& s) {
+  unsigned long long sda = (unsigned long long)s.a * s.x + s.y;
+  s.x = (uint32_t)sda;
+  s.y = (uint32_t)(sda >> 32);
+  const float f = __uint_as_float((s.x >> 9) | 0x3f800000u);
+  return fmaf(-2 * FPI, f, 4 * FPI);
+}
+
 // gpu/pro.cu:87-95
 __device__ __forceinline__ float grnd(Rng& s) {
   float a = sqrtf(-2 * logf(xrnd(s)));
-  return a * sinf(2 * FPI * xrnd(s));
+  return a * sinf(xrnd_angle(s));
 }
 
 __device__ __forceinline__ float2 grnd2(Rng& s) {
   float r = sqrtf(-2 * logf(xrnd(s)));
   float2 p;
-  sincosf(2 * FPI * xrnd(s), &p.y, &p.x);
+  sincosf(xrnd_angle(s), &p.y, &p.x);
   return __fmul2_rn(p, make_float2(r, r));
 }
 
@@ -159,7 +169,7 @@ __device__ __forceinline__ void rotate(float cs, float si, float4& n, Rng& s) {
   }
   {
     float2 p;
-    float xi = 2 * FPI * xrnd(s);
+    float xi = xrnd_angle(s);
     sincosf(xi, &p.y, &p.x);
     n.x -= cs * n.x - si * (p.x * p1.x + p.y * p2.x);
     n.y -= cs * n.y - si * (p.x * p1.y + p.y * p2.y);
