@@ -162,10 +162,17 @@ class PPC:
         return f(a), f(b)
 
     # ---- direct hot path -----------------------------------------------------------
-    def propagate(self, bunches, cap=1 << 22):
-        """Host bunches in, kernel-level hits out (copies included)."""
+    def propagate(self, bunches, cap=1 << 22, out=None):
+        """Host bunches in, kernel-level hits out (copies included).  `out`: a caller-owned
+        HIT_DTYPE array that receives the hits (its length is the capacity); the result is
+        a view of it."""
         bunches = np.ascontiguousarray(bunches, T.BUNCH_DTYPE)
-        hits = np.empty(cap, T.HIT_DTYPE)  # only the first min(produced, cap) records are written
+        if out is not None:
+            if out.dtype != T.HIT_DTYPE or not out.flags.c_contiguous:
+                raise TypeError("out must be a contiguous HIT_DTYPE array")
+            hits, cap = out, len(out)
+        else:
+            hits = np.empty(cap, T.HIT_DTYPE)  # only the first min(produced, cap) records are written
         nh = C.c_uint64()
         info = RunInfo()
         check(lib().ppcb_propagate(self._c, _p(bunches), len(bunches), _p(hits), cap, C.byref(nh), C.byref(info)))

@@ -1,6 +1,7 @@
 // C ABI over Session / Engine (declarations and reference citations: include/ppc_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -269,18 +270,17 @@ int ppcb_propagate(ppcb_ctx* c, const ppcb_bunch* bunches, int32_t nb, ppcb_hit*
     if (!e.ready()) throw ppcb::Error("ppcb_ini() must come before propagation", PPCB_ESTATE);
     ppcb::RunInfo tot;
     uint64_t produced = 0, stored = 0;
-    std::vector<ppcb_hit> got;
+    // kept hits go from the pinned staging buffer straight into the caller's array
+    auto sink = [&](const ppcb_hit* h, uint64_t n) {
+      if (hits && stored < cap) std::memcpy(hits + stored, h, std::min<uint64_t>(n, cap - stored) * sizeof(ppcb_hit));
+      stored += n;
+    };
     auto drain_one = [&]() {
       ppcb::RunInfo ri;
-      got.clear();
-      e.collect(got, ri);
+      e.collect(sink, ri);
       tot.photons += ri.photons; tot.hits += ri.hits; tot.kept += ri.kept; tot.steps += ri.steps;
       tot.nan_steps += ri.nan_steps; tot.capped += ri.capped; tot.device_ms += ri.device_ms;
       produced += ri.hits;
-      for (auto& h : got) {
-        if (stored < cap && hits) hits[stored] = h;
-        stored++;
-      }
     };
     // batches of at most pmax photons and pmxo bunches (gpu/f2k.cxx:377-385)
     std::vector<ppcb_bunch> batch;

@@ -296,6 +296,10 @@ long Engine::submit(const ppcb_bunch* b, int nb, uint64_t num) {
 }
 
 bool Engine::collect(std::vector<ppcb_hit>& out, RunInfo& info, long* tagp) {
+  return collect([&](const ppcb_hit* h, uint64_t n) { out.insert(out.end(), h, h + n); }, info, tagp);
+}
+
+bool Engine::collect(const std::function<void(const ppcb_hit*, uint64_t)>& sink, RunInfo& info, long* tagp) {
   if (queue_.empty()) return false;
   long tag = queue_.front();
   queue_.pop_front();
@@ -321,7 +325,7 @@ bool Engine::collect(std::vector<ppcb_hit>& out, RunInfo& info, long* tagp) {
     if (kept) {
       check(cudaMemcpyAsync(g.hhits, S->hits, kept * sizeof(ppcb_hit), cudaMemcpyDeviceToHost, g.cp), "D2H hits");
       check(cudaStreamSynchronize(g.cp), "D2H hits");
-      out.insert(out.end(), g.hhits, g.hhits + kept);
+      sink(g.hhits, kept);
     }
     info.photons += S->num;
     info.hits += c.hidx;

@@ -9,6 +9,7 @@
 #include <deque>
 #include <memory>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "config.h"
@@ -102,6 +103,9 @@ class Engine {
   long submit(const ppcb_bunch* b, int nb, uint64_t num);
   // Wait for the oldest queued batch; append its kept hits.  False if none queued.
   bool collect(std::vector<ppcb_hit>& out, RunInfo& info, long* tag = nullptr);
+  // The same, handing each device's kept hits to `sink` straight from the pinned staging
+  // buffer (valid during the call only).
+  bool collect(const std::function<void(const ppcb_hit*, uint64_t)>& sink, RunInfo& info, long* tag = nullptr);
   int in_flight() const { return (int)queue_.size(); }
 
   // Device-pointer entry point: one launch on device `d` over caller buffers.

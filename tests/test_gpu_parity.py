@@ -287,3 +287,27 @@ def test_device_entry_point_matches_host_path(ice_small):
     assert cc.hidx == info["hits"] == len(hh)
     assert np.array_equal(np.sort(hd, order=["i", "t"]), np.sort(hh, order=["i", "t"]))
     c.close()
+
+
+def test_propagate_into_caller_buffer(ice_small):
+    """PPC.propagate(out=...) writes into the caller's array: the same hits as a run into a
+    library-allocated one (same seed, photon i on thread i mod T), and with a smaller array
+    the first len(out) records, while the reported count stays the full one."""
+    tmpl = T.bunch_led([0, 0, 0, 0], [0, 0, 1], 3, 400000, 1, ka=-1, up=0, fldr=-1)
+    c = _ctx(ice_small, seed=3, deterministic=True)
+    h1, i1 = c.propagate(tmpl)
+    assert len(h1) > 100
+    key = lambda h: np.sort(h.view(np.uint8).reshape(len(h), -1).view("V32").ravel())
+    c.set_seed(3)
+    out = np.zeros(len(h1) + 10, T.HIT_DTYPE)
+    h2, i2 = c.propagate(tmpl, out=out)
+    assert np.shares_memory(h2, out) and i2["hits"] == i1["hits"] and len(h2) == len(h1)
+    assert np.array_equal(key(h1), key(h2))
+    c.set_seed(3)
+    small = np.zeros(len(h1) // 3, T.HIT_DTYPE)
+    h3, i3 = c.propagate(tmpl, out=small)
+    assert i3["hits"] == i1["hits"] and len(h3) == len(small)
+    assert np.isin(key(h3), key(h1)).all()
+    with pytest.raises(TypeError):
+        c.propagate(tmpl, out=np.zeros(10, np.float32))
+    c.close()
