@@ -149,6 +149,20 @@ def test_propagation_before_ini_is_an_error(ice_small):
     c.close()
 
 
+def test_result_array_must_be_hit_records(ice_small):
+    """PPC.propagate(out=...) takes only a contiguous array of hit records (checked before
+    any work is done)."""
+    import numpy as np
+    from ppc_b200 import types as T
+    c = PPC()
+    c.initialize(1.0, ice_small)
+    b = T.bunch_led([0, 0, 0, 0], [0, 0, 1], 1, 10, 1, ka=-1, up=0, fldr=-1)
+    for bad in (np.zeros(10, np.float32), np.zeros(20, T.HIT_DTYPE)[::2]):
+        with pytest.raises(TypeError):
+            c.propagate(b, out=bad)
+    c.close()
+
+
 def test_flasher_setup_matches_reference_semantics(ice_full, monkeypatch):
     """flset/fldir/flshift are host-side (gpu/f2k.cxx:590-765)."""
     monkeypatch.setenv("FLDR", "30")
