@@ -48,7 +48,6 @@ struct SmemTables {
   uint16_t ls[PPCB_NSTR];
   uint16_t is[PPCB_CX * PPCB_CY];
   int8_t mcol[PPCB_CTX * PPCB_CTY];
-  float4 bfrt[PPCB_BFR_TAB + 1];  // birefringence angular functions (sx, sy, mx, -)
   StrGroup sgg[PPCB_NSTR + 1];    // string-proximity table: string axes and the sentinel (strgrid.h)
   float4 azr[PPCB_MAXLYS];        // per layer 1/k1, 1/k2, 1/(k1 k2): the scattering's frame divisions
   float4 scat[2][2];              // bulk [0] / hole ice [1]: (sf, g, gr, 1/(1-sf)), (1-g^2, (1-g)^2, 1/(2g), 1/sf)
@@ -607,6 +606,15 @@ __device__ __noinline__ void record_nan_step(const KArgs& a) {
   if (k < 4) { unsigned int sm; asm volatile("mov.u32 %0, %%smid;" : "=r"(sm)); a.ctrl->bad_sm[k] = sm; }
 }
 
+// Tables in dynamic shared memory (load_dyn): the string-proximity cells and the
+// birefringence angular functions per interval.
+constexpr size_t kBfrBytes = PPCB_BFR_TAB * (sizeof(float4) + sizeof(float2));
+struct DynTabs {
+  const uint16_t* cells;
+  const float4* bfr0;
+  const float2* bfr1;
+};
+
 // String-proximity table as the kernel reads it: cell entries in dynamic shared memory,
 // string axes in the static tables.
 struct SgTab {
@@ -698,7 +706,7 @@ __device__ __forceinline__ Found dom_search(const KArgs& a, const SmemTables& S,
 // gpu/pro.cu:499-888: one propagation step (one scattering segment).  Returns with
 // ph.TOT == 0 once the photon is absorbed or registered.
 template <class HOOK>
-__device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const uint16_t* sgc, Photon& ph, Rng& s,
+__device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const DynTabs& dt, Photon& ph, Rng& s,
                                      unsigned int& nan_steps, HOOK& hk) {
   const ppcb_params& e = a.p;
   const float2* __restrict__ wz = a.absca + (size_t)ph.wl * e.size;
@@ -773,7 +781,7 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
   // DOM search, gpu/pro.cu:577-672: only for the steps that may reach a string's cylinder
   // (strgrid.h; on the full detector about 0.2% of them); for the others it would find
   // nothing and leave om, del, hi, hf and sqd as they are
-  if (sg_may_reach(a.sg, SgTab{S, sgc}, r.x, r.y, n.x, n.y, n.z, sca)) {
+  if (sg_may_reach(a.sg, SgTab{S, dt.cells}, r.x, r.y, n.x, n.y, n.z, sca)) {
     const Found f = dom_search(a, S, r, n, sca, old, ph.ofla);
     om = f.om; del = f.del; hi = f.hi; hf = f.hf; sqd = f.sqd;
   }
@@ -841,12 +849,11 @@ __device__ __forceinline__ void step(const KArgs& a, const SmemTables& S, const 
         const float v = sqrtf(fmaxf(0.f, 1.f - fabsf(dot))) * PPCB_BFR_TAB;
         const int iv = min((int)v, PPCB_BFR_TAB - 1);
         const float fv = v - iv;
-        const float4 t0 = S.bfrt[iv], t1 = S.bfrt[iv + 1];
+        const float4 t0 = dt.bfr0[iv];
+        const float2 d01 = dt.bfr1[iv];
         const float sra = sqrtf(ra);
-        const float2 a0 = make_float2(t0.x, t0.y);
-        const float2 d01 = __fadd2_rn(make_float2(t1.x, t1.y), make_float2(-t0.x, -t0.y));
-        sxy = __fmul2_rn(make_float2(sra, sra), __ffma2_rn(make_float2(fv, fv), d01, a0));
-        mx = rb * fmaf(fv, t1.z - t0.z, t0.z);
+        sxy = __fmul2_rn(make_float2(sra, sra), __ffma2_rn(make_float2(fv, fv), d01, make_float2(t0.x, t0.y)));
+        mx = rb * fmaf(fv, t0.w, t0.z);
       }
       const float sg = dot < 0 ? -1.f : 1.f;
       float2 qxy = __fmul2_rn(__ffma2_rn(make_float2(-dot, -dot), nxy, make_float2(e.azx, e.azy)), make_float2(sg, sg));
@@ -942,7 +949,6 @@ __device__ __forceinline__ void load_tables(const KArgs& a, SmemTables& S) {
   for (int i = t; i < PPCB_NSTR; i += nt) S.ls[i] = a.ls[i];
   for (int i = t; i < PPCB_CX * PPCB_CY; i += nt) S.is[i] = a.is[i];
   for (int i = t; i < PPCB_CTX * PPCB_CTY; i += nt) S.mcol[i] = a.mcol[i];
-  for (int i = t; i <= PPCB_BFR_TAB; i += nt) S.bfrt[i] = a.bfrt[i];
   for (int i = t; i < a.sg_ngroups; i += nt) S.sgg[i] = a.sg_groups[i];
   if (t < 2) {
     const float sf = t ? a.p.SF : a.p.sf, g = t ? a.p.G : a.p.g, gr = t ? a.p.GR : a.p.gr;
@@ -965,6 +971,23 @@ __device__ __forceinline__ void load_cells(const KArgs& a, uint16_t* cells) {
   const int n = a.sg.on ? a.sg.nx * a.sg.ny : 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) cells[i] = a.sg_cells[i];
   __syncthreads();
+}
+
+// Tables in dynamic shared memory: the string-proximity cells, then the birefringence
+// angular functions per interval as (sx, sy, mx, next mx - mx) and (next sx - sx,
+// next sy - sy): one 16-byte and one 8-byte load per step, and the differences the
+// interpolation needs rounded once here instead of every step (the same floats).
+__device__ __forceinline__ DynTabs load_dyn(const KArgs& a, unsigned char* base) {
+  uint16_t* cells = reinterpret_cast<uint16_t*>(base);
+  float4* b0 = reinterpret_cast<float4*>(base + sg_cells_bytes(a));
+  float2* b1 = reinterpret_cast<float2*>(base + sg_cells_bytes(a) + PPCB_BFR_TAB * sizeof(float4));
+  for (int i = threadIdx.x; i < PPCB_BFR_TAB; i += blockDim.x) {
+    const float4 t0 = a.bfrt[i], t1 = a.bfrt[i + 1];
+    b0[i] = make_float4(t0.x, t0.y, t0.z, __fsub_rn(t1.z, t0.z));
+    b1[i] = make_float2(__fsub_rn(t1.x, t0.x), __fsub_rn(t1.y, t0.y));
+  }
+  load_cells(a, cells);
+  return DynTabs{cells, b0, b1};
 }
 
 #define PPCB_BLOCK 256
@@ -1002,11 +1025,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
   extern __shared__ __align__(16) unsigned char dsm[];
   PhotonPool<STREAMS>* pools = reinterpret_cast<PhotonPool<STREAMS>*>(dsm);
   Prov* snaps = reinterpret_cast<Prov*>(dsm + (BLOCK / 32) * sizeof(PhotonPool<STREAMS>));
-  uint16_t* sgc = reinterpret_cast<uint16_t*>(dsm + dyn_smem<BLOCK, REC, STREAMS>());
   __shared__ unsigned long long bsteps;  // the block's propagation steps
   if (threadIdx.x == 0) bsteps = 0;
   load_tables(a, S);
-  load_cells(a, sgc);
+  const DynTabs dt = load_dyn(a, dsm + dyn_smem<BLOCK, REC, STREAMS>());
   // launch sizes: from the parameters, or from device memory for replayed graphs
   const uint64_t num = a.dyn ? a.dyn[0] : a.num;
   const int nb = a.dyn ? (int)a.dyn[1] : a.nb;
@@ -1136,7 +1158,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_propagate(const __grid_constant
       continue;
     }
     if (alive) {
-      step(a, S, sgc, ph, s, nan_steps, hk);
+      step(a, S, dt, ph, s, nan_steps, hk);
       ph.steps++;
       if (a.max_steps && ph.steps >= a.max_steps && ph.TOT != 0) {  // the step cap (rare)
         ph.TOT = 0;
@@ -1176,10 +1198,9 @@ __global__ void __launch_bounds__(256, 3) k_adjoint(const __grid_constant__ KArg
   __shared__ SmemTables S;
   __shared__ double gbe[PPCB_MAXLYS], gba[PPCB_MAXLYS];
   extern __shared__ __align__(16) unsigned char dsm[];
-  uint16_t* sgc = reinterpret_cast<uint16_t*>(dsm);
   for (int i = threadIdx.x; i < PPCB_MAXLYS; i += blockDim.x) { gbe[i] = 0; gba[i] = 0; }
   load_tables(a, S);
-  load_cells(a, sgc);
+  const DynTabs dt = load_dyn(a, dsm);
   unsigned int nan_steps = 0, replayed = 0, unmatched = 0;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nh; k += (uint64_t)gridDim.x * blockDim.x) {
     const ppcb_hit h = hits[k];
@@ -1213,7 +1234,7 @@ __global__ void __launch_bounds__(256, 3) k_adjoint(const __grid_constant__ KArg
     hk.prov_out = nullptr;
     hk.start = nullptr;
     while (!hk.done && ph.TOT != 0 && ph.steps < a.max_steps) {
-      step(a, S, sgc, ph, s, nan_steps, hk);
+      step(a, S, dt, ph, s, nan_steps, hk);
       ph.steps++;
     }
     replayed++;
@@ -1247,7 +1268,7 @@ cudaError_t adjoint_prepare() {
   if (e != cudaSuccess) return e;
   if (!(done.load() & (1ull << (dev & 63)))) {
     e = cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(kSgMaxCells * sizeof(uint16_t)));
+                             (int)(kSgMaxCells * sizeof(uint16_t) + kBfrBytes));
     if (e != cudaSuccess) return e;
     done.fetch_or(1ull << (dev & 63));
   }
@@ -1260,7 +1281,7 @@ cudaError_t launch_adjoint(const KArgs& a, const ppcb_hit* hits, const void* pro
   if (nh == 0) return cudaSuccess;
   const cudaError_t e = adjoint_prepare();
   if (e != cudaSuccess) return e;
-  k_adjoint<<<blocks, 256, sg_cells_bytes(a), st>>>(a, hits, static_cast<const Prov*>(prov), nh, nh_dev, events,
+  k_adjoint<<<blocks, 256, sg_cells_bytes(a) + kBfrBytes, st>>>(a, hits, static_cast<const Prov*>(prov), nh, nh_dev, events,
                                                    wdom, wgrad, g_out, stats);
   return cudaGetLastError();
 }
@@ -1330,8 +1351,8 @@ __global__ void k_index_probe(const __grid_constant__ KArgs a, const float4* pos
 // string-proximity cell entries; the attribute allows the largest table.
 template <int BLOCK, int MINB, bool REC, bool STREAMS>
 static cudaError_t launch_one(const KArgs& a, int blocks, cudaStream_t st) {
-  constexpr size_t dmax = dyn_smem<BLOCK, REC, STREAMS>() + kSgMaxCells * sizeof(uint16_t);
-  const size_t dyn = dyn_smem<BLOCK, REC, STREAMS>() + sg_cells_bytes(a);
+  constexpr size_t dmax = dyn_smem<BLOCK, REC, STREAMS>() + kSgMaxCells * sizeof(uint16_t) + kBfrBytes;
+  const size_t dyn = dyn_smem<BLOCK, REC, STREAMS>() + sg_cells_bytes(a) + kBfrBytes;
   if (dyn > dmax) return cudaErrorInvalidValue;
   static std::atomic<uint64_t> done{0};
   int dev = 0;
@@ -1403,7 +1424,7 @@ cudaError_t propagate_attributes(int* regs, int* max_threads, size_t* smem, size
 template <int BLOCK, int MINB>
 static int max_blocks(int* nb) {
   // the larger pool (per-photon streams) and the largest string-proximity table
-  constexpr size_t dyn = dyn_smem<BLOCK, false, true>() + kSgMaxCells * sizeof(uint16_t);
+  constexpr size_t dyn = dyn_smem<BLOCK, false, true>() + kSgMaxCells * sizeof(uint16_t) + kBfrBytes;
   cudaError_t e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, false, false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_propagate<BLOCK, MINB, false, false>, BLOCK, dyn);
@@ -1414,7 +1435,7 @@ static int max_blocks(int* nb) {
 // largest string-proximity table included); 0 when the shape does not fit.
 template <int BLOCK, int MINB, bool STREAMS>
 static int rec_blocks(int* nb) {
-  constexpr size_t dyn = dyn_smem<BLOCK, true, STREAMS>() + kSgMaxCells * sizeof(uint16_t);
+  constexpr size_t dyn = dyn_smem<BLOCK, true, STREAMS>() + kSgMaxCells * sizeof(uint16_t) + kBfrBytes;
   cudaError_t e = cudaFuncSetAttribute(k_propagate<BLOCK, MINB, true, STREAMS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e == cudaSuccess)
